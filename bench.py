@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Throughput of the spektri filter bank + Welch spectrum on B200.
+
+Metric: input Msamples/s.  Workload (default): the batching configuration —
+a real int16 stream at 64.8 MS/s, forward FFT 65536 with 25 % overlap, Welch
+average over 256 blocks, 256 channels with IFFT sizes 64..8192 and taper
+widths 8..64, 64 blocks per buffer.  A step is one buffer (64 blocks,
+3,145,728 new samples) through the whole path: forward FFTs, Welch terms and
+accumulation, and the filter bank (one persistent launch).
+
+  value : device-resident input and outputs, CUDA events on the launching
+          stream over K steps (max over ranks), inputs cycled over more than
+          L2 of distinct buffers and outputs (200 MB/step) larger than L2.
+  e2e   : the public host API (sk_process): pinned host input copied in, all
+          channel outputs and spectra copied back, every step.
+  roofline: the filter-bank kernel, algorithmic bytes (its channel outputs)
+          per launch / its event-timed launch duration, against the measured
+          HBM copy bandwidth.
+  cpu_baseline: the FP32 CPU restatement of the reference path on this host's
+          cores, on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU restatement alone (the reference arm:
+the Rust reference cannot be built without a Rust toolchain).
+Multi-GPU (torchrun): each rank processes its own stream of the same
+configuration (replicas, weak scaling); no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DISTINCT_BUFFERS = 48          # 48 x 6.3 MB of input cycled: 302 MB > 126 MB L2
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, ws, local):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(w, raws, seconds, threads):
+    """The FP32 CPU restatement on a bounded sample: whole buffers of the same
+    workload until ``seconds`` of work (at least 2 buffers)."""
+    from oracle import oracle32
+    o = oracle32.Oracle32(w.fs, w.fc, w.fft_size, w.ffts_per_buf, w.averages, w.fmt, w.filters(),
+                          spectrum_format="f32", n_threads=threads)
+    o.process(raws[0])                        # warm-up (thread start, page faults)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.process(raws[n % len(raws)])
+        n += 1
+        dt = time.perf_counter() - t0
+        if (dt >= seconds and n >= 2) or n >= 400:
+            break
+    return n * w.samples_per_buffer / dt, n
+
+
+def run_reference(args, ws, rank):
+    """Reference arm: the CPU restatement with all host threads, on this
+    workload's configuration; each step one bounded sample (a buffer)."""
+    if rank != 0:
+        return
+    from spektri_b200 import workloads
+    from oracle import oracle32
+    w = workloads.WORKLOADS[args.workload]()
+    threads = len(os.sched_getaffinity(0))
+    per_buf = w.samples_per_buffer
+    raw = workloads.stream_numpy(w, 0, 2 * per_buf)
+    raws = [r.view(np.uint8) for r in np.split(raw, 2)]
+    o = oracle32.Oracle32(w.fs, w.fc, w.fft_size, w.ffts_per_buf, w.averages, w.fmt, w.filters(),
+                          spectrum_format="f32", n_threads=threads)
+    for i in range(args.warmup):
+        o.process(raws[i % 2])
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        o.process(raws[i % 2])
+    dt = time.perf_counter() - t0
+    v = args.steps * per_buf / dt / 1e6
+    line = {
+        "impl": "reference", "metric": "input Msamples/s", "value": round(v, 3), "unit": "Msamples/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.name, "fft_size": w.fft_size, "channels": len(w.channels),
+                   "ffts_per_buf": w.ffts_per_buf, "input": w.fmt},
+        "cpu_baseline": {"value": round(v, 3), "unit": "Msamples/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} buffers of {per_buf} samples (FP32 C++ restatement; the Rust "
+                                   f"reference needs a Rust toolchain, absent here)"},
+        "e2e": {"value": round(v, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--compare-plain", action="store_true", help="also time the plain per-channel path")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+
+    import torch
+    from spektri_b200 import Plan, pinned_empty, workloads
+
+    dev = local
+    torch.cuda.set_device(dev)
+    w = workloads.WORKLOADS[args.workload]()
+    w.seed += 7919 * rank                                 # each replica its own stream
+    spb = w.samples_per_buffer
+    nbuf = min(DISTINCT_BUFFERS, w.n_samples // spb)
+    stream_dev = workloads.stream_torch(w, nbuf * spb, f"cuda:{dev}")
+    raw_bytes = spb * w.bytes_per_sample
+    raws = [stream_dev[i * raw_bytes:(i + 1) * raw_bytes] for i in range(nbuf)]
+
+    def make(mode):
+        return Plan(w.fs, w.fft_size, w.fmt, w.filters(), fc_in=w.fc, ffts_per_buf=w.ffts_per_buf,
+                    averages=w.averages, spectrum_format="f32", mode=mode, device=dev)
+
+    plan = make(args.mode)
+    outs = [torch.empty(c["out_samples"], dtype=torch.complex64, device=dev) for c in plan.channels]
+    spec = torch.empty(plan.max_spectra * plan.spectrum_bytes, dtype=torch.uint8, device=dev)
+    st = torch.cuda.Stream(dev)
+
+    def run_steps(p, k, start):
+        with torch.cuda.stream(st):
+            for i in range(k):
+                p.process_device(raws[(start + i) % nbuf], outs, spec, stream=st)
+
+    run_steps(plan, args.warmup, 0)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    run_steps(plan, args.steps, args.warmup)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, ws, local)
+    value = args.steps * spb * ws / (ms_max / 1e3) / 1e6       # Msamples/s, all ranks
+
+    # Per-stage event timing (same stream, same work), for the roofline.
+    plan.set_timing(True)
+    kt = min(args.steps, 50)
+    run_steps(plan, kt, 0)
+    stage_ms, calls = plan.timing()
+    plan.set_timing(False)
+    fcfb_ms = stage_ms[3] / max(1, calls)
+    out_bytes = sum(c["out_samples"] for c in plan.channels) * 8
+    hbm, peak_kind = peaks()
+    achieved = out_bytes / (fcfb_ms / 1e3) / 1e9
+    alg = w.alg_bytes_per_sample()
+    result = {
+        "metric": "input Msamples/s", "value": round(value, 2), "unit": "Msamples/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded int16 noise + tones + noise carriers, generated on the GPU)",
+        "config": {"workload": w.name, "mode": args.mode, "input": w.fmt, "fs": w.fs, "fft_size": w.fft_size,
+                   "ffts_per_buf": w.ffts_per_buf, "averages": w.averages, "channels": len(w.channels),
+                   "sum_ifft_bins": sum(c["n"] for c in w.channels), "samples_per_step": spb,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": f"{nbuf} distinct input buffers cycled ({nbuf * raw_bytes / 1e6:.0f} MB) and "
+                         f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2"},
+        "hbm_gbs_pipeline": round(value * 1e6 / ws * alg / 1e9, 1),
+        "alg_bytes_per_sample": round(alg, 3),
+        "stage_ms": {k: round(v / max(1, calls), 4) for k, v in zip(["fwd_fft", "welch_split", "welch_accum", "fcfb"], stage_ms)},
+        "roofline": {"bound": "hbm", "kernel": "fcfb_kernel (persistent)", "achieved": round(achieved, 1),
+                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "peak_kind": f"{peak_kind} copy bandwidth", "traffic": None,
+                     "alg_bytes_per_launch": out_bytes, "launch_ms": round(fcfb_ms, 4)},
+        "gpu_launches": plan.launches_per_call * args.steps,
+        "clocks": clk,
+    }
+    prof = os.path.join(ROOT, "profiles", "fcfb_traffic.json")
+    if os.path.exists(prof):
+        d = json.load(open(prof))
+        if d.get("workload") == w.name and d.get("kernel") == "fcfb_kernel":
+            result["roofline"]["traffic"] = d.get("dram_bytes_per_launch")
+
+    if args.compare_plain and args.mode == "batched":
+        pp = make("plain")
+        run_steps(pp, args.warmup, 0)
+        torch.cuda.synchronize(dev)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
+        kp = min(args.steps, 50)
+        run_steps(pp, kp, 0)
+        a1.record(st)
+        torch.cuda.synchronize(dev)
+        vp = kp * spb / (a0.elapsed_time(a1) / 1e3) / 1e6
+        result["plain_value"] = round(vp, 2)
+        result["batched_over_plain"] = round(value / ws / vp, 2)
+        del pp
+
+    # End to end through the public host API, with pinned host buffers.
+    ke = max(1, min(args.e2e_steps, args.steps))
+    nin = 4
+    hin = [pinned_empty((raw_bytes,), np.uint8) for _ in range(nin)]
+    for i in range(nin):
+        hin[i][:] = raws[i].cpu().numpy()
+    houts, hspec = plan.empty_outputs(pinned=True)
+    plan.process_into(hin[0], houts, hspec)               # warm-up
+    d2h = 0
+    barrier(ws)
+    t0 = time.perf_counter()
+    for i in range(ke):
+        r = plan.process_into(hin[i % nin], houts, hspec)
+        d2h += out_bytes + r.n_spectra * plan.spectrum_bytes
+    dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt, ws, local)
+    result["e2e"] = {"value": round(ke * spb * ws / dt / 1e6, 2), "unit": "Msamples/s",
+                     "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": int(d2h / ke)}
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = len(os.sched_getaffinity(0))
+        raws_h = [hin[i].copy() for i in range(2)]
+        v, n = cpu_baseline(w, raws_h, args.cpu_seconds, threads)
+        result["cpu_baseline"] = {"value": round(v / 1e6, 3), "unit": "Msamples/s", "cores": threads,
+                                  "kind": "port",
+                                  "sample": f"{n} buffers x {spb} samples of the same workload, FP32 C++ "
+                                            f"restatement, {threads} threads"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    barrier(ws)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * spektri_b200 — C ABI of the B200 (sm_100a) fast-convolution filter bank and
+ * Welch spectrum.
+ *
+ * The reference (tejeez/spektri) is a single Rust binary; the seam this ABI
+ * replaces is its DSP state machine:
+ *
+ *   DspState::init(DspParams) -> (DspState, InputBufferSize)   spektri/src/dsp.rs:76-111
+ *   DspState::process_real / process_complex                   spektri/src/dsp.rs:114-160
+ *   MultiFft::process_real / process_complex                   spektri/src/dsp/multifft.rs:34-95
+ *   SpectrumAccumulator::accumulate                            spektri/src/dsp/spectrum.rs:82-163
+ *   Fcfb::add_filter / Fcfb::process / FilterDsp::process      spektri/src/dsp/fcfb.rs:41-188
+ *   freq_to_bins / bins_to_freq / freq_to_bins_exact           spektri/src/dsp/fcfb.rs:225-285
+ *   serialize_metadata / serialize_*_topic                     spektri/src/dsp/data.rs:110-171
+ *   convert_to_f32 / convert_to_cf32 (fused into the FFT load)  spektri/src/inputformats.rs:65-155
+ *
+ * Conventions.  Every function returns an int status (SK_OK = 0, negative =
+ * error, positive = warning) and never aborts; sk_last_error() gives the
+ * message of the last failure on the calling thread.  A plan is driven by one
+ * host thread at a time (the reference keeps all I/O on its main thread,
+ * spektri/src/dsp/output.rs:1-6).  The caller owns raw input and output
+ * buffers; the plan owns all device state (the N/4 sample halo, the Welch
+ * accumulator, twiddles, weights and scratch).  Complex samples are
+ * interleaved float32 (re, im) — the complex64 wire format of fcfb.rs:180-187.
+ */
+#ifndef SPEKTRI_B200_H
+#define SPEKTRI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define SK_OK               0
+#define SK_WARN_FILTER      1   /* plan made; some filters were dropped, as fcfb.rs:58-61 does */
+#define SK_ERR_ARG         -1   /* invalid argument (the reference would panic or clap would exit) */
+#define SK_ERR_FILTER      -2   /* filter parameters not exactly representable (fcfb.rs:274-285) */
+#define SK_ERR_CUDA        -3   /* a CUDA runtime call failed */
+#define SK_ERR_NOMEM       -4   /* device or pinned host allocation failed */
+#define SK_ERR_TIMEOUT     -5   /* a bounded device wait gave up */
+#define SK_ERR_UNSUPPORTED -6   /* valid for the reference, not implemented on the device path */
+#define SK_ERR_STATE       -7   /* call out of order */
+
+/* ------------------------------------------------------------ enums */
+/* Input sample formats: the DataFormat codes of spektri/src/dsp/data.rs:79-96. */
+enum {
+  SK_FMT_S8 = 0x04, SK_FMT_S16LE = 0x08, SK_FMT_S16BE = 0x09, SK_FMT_F32LE = 0x1C,
+  SK_FMT_F32BE = 0x1D, SK_FMT_U8 = 0x24, SK_FMT_CS8 = 0x44, SK_FMT_CS16LE = 0x48,
+  SK_FMT_CS16BE = 0x49, SK_FMT_CF32LE = 0x5C, SK_FMT_CF32BE = 0x5D, SK_FMT_CU8 = 0x64
+};
+/* Spectrum record formats: SpectrumFormat of spectrum.rs:29-32 (u8 at
+ * 0.5 dB/LSB, u16 big-endian at 0.05 dB/LSB) plus f32 mean power acc/accn. */
+enum { SK_SPEC_U8 = 0, SK_SPEC_U16 = 1, SK_SPEC_F32 = 2 };
+/* Filter-bank execution: one launch per channel, or every channel in one
+ * persistent size-ordered launch per buffer, replayed from a CUDA graph. */
+enum { SK_MODE_PLAIN = 0, SK_MODE_BATCHED = 1 };
+
+/* ------------------------------------------------------------ structures */
+/* DspParams (dsp.rs:22-33) plus device selection. */
+typedef struct {
+  double   fs_in;            /* --samplerate */
+  double   fc_in;            /* --centerfreq */
+  uint32_t fft_size;         /* --fftsize, N */
+  uint32_t ffts_per_buf;     /* --fftbuf, B (even for real input: multifft.rs:57-61) */
+  uint32_t averages;         /* --averages */
+  int32_t  input_format;     /* --inputformat, SK_FMT_* */
+  int32_t  spectrum_format;  /* --spectrumformat, SK_SPEC_* */
+  int32_t  mode;             /* SK_MODE_* */
+  int32_t  device;           /* CUDA device ordinal */
+  uint32_t flags;            /* reserved, must be 0 */
+} sk_params;
+
+/* FilterParams (fcfb.rs:206-210) plus weight design. */
+typedef struct {
+  double       fs_out;       /* fs= : output sample rate */
+  double       fc_out;       /* fc= : output centre frequency */
+  const float* weights;      /* w= : complex64[bins] on the host, W[j] scales bin first+j;
+                                NULL selects designed real weights (below) */
+  uint32_t     transition;   /* tw= : with weights==NULL, Tukey taper of this many bins per
+                                side; 0 keeps the reference's raised cosine (fcfb.rs:197-203) */
+  uint32_t     reserved;
+} sk_filter;
+
+/* InputBufferSize (dsp.rs:36-40) plus output sizing. */
+typedef struct {
+  uint64_t new_samples;      /* samples consumed per sk_process call: 3N/4 * B */
+  uint64_t overlap;          /* N/4, carried inside the plan */
+  uint64_t total;            /* new + overlap */
+  uint64_t raw_bytes;        /* bytes of raw input per call */
+  uint32_t result_bins;      /* K: N/2+1 (real) or N (complex) */
+  uint32_t n_channels;       /* filters that passed validation, in their given order */
+  uint32_t max_spectra;      /* upper bound on spectrum records per call */
+  uint32_t spectrum_bytes;   /* payload bytes of one spectrum record (no metadata) */
+} sk_plan_info;
+
+typedef struct {
+  uint32_t bins;             /* IFFT size n (BinNumbers.bins) */
+  int32_t  filter_index;     /* position in the sk_filter array given at creation */
+  int64_t  first;            /* first bin (BinNumbers.first) */
+  double   fs_out, fc_out;
+  uint64_t out_samples;      /* complex64 samples per call: B * 3n/4 */
+} sk_channel_info;
+
+typedef struct {
+  uint32_t n_spectra;        /* spectrum records completed in this call */
+  uint32_t reserved;
+  uint64_t spectrum_seq0;    /* sequence number of the first one (spectrum.rs:36,160) */
+} sk_result;
+
+typedef struct sk_plan sk_plan;
+
+/* ------------------------------------------------------------ host-only helpers
+ * These need no GPU.  Bit-exact with the reference's f64 arithmetic. */
+
+/* freq_to_bins (fcfb.rs:225-252).  SK_ERR_FILTER when bins <= 0. */
+int sk_freq_to_bins(double fs_in, double fc_in, uint64_t fft_size, double fs_out, double fc_out,
+                    uint32_t* bins, int64_t* first);
+/* freq_to_bins_exact (fcfb.rs:274-285).  SK_ERR_FILTER unless the round trip is exact. */
+int sk_freq_to_bins_exact(double fs_in, double fc_in, uint64_t fft_size, double fs_out, double fc_out,
+                          uint32_t* bins, int64_t* first);
+/* bins_to_freq (fcfb.rs:257-268). */
+int sk_bins_to_freq(double fs_in, double fc_in, uint64_t fft_size, uint32_t bins, int64_t first,
+                    double* fs_out, double* fc_out);
+/* raised_cosine_weights (fcfb.rs:197-203) as complex64 with zero imaginary parts. */
+int sk_raised_cosine_weights(uint32_t n, float* out_c64);
+/* Periodic Tukey weights, tw taper bins per side (prototyping/fcfb.py:122). */
+int sk_tukey_weights(uint32_t n, uint32_t tw, float* out_c64);
+/* serialize_metadata (data.rs:110-132): 24 bytes <u64 seq, u64 secs, u32 nanos, u32 0>. */
+int sk_serialize_metadata(uint8_t out[24], uint64_t seq, uint64_t secs, uint32_t nanos);
+/* serialize_signal_topic (data.rs:137-153): [2, 0x40, 0x5C, 0 x5, f64 fs, f64 fc]. */
+int sk_signal_topic(uint8_t out[24], double fs, double fc);
+/* serialize_spectrum_topic (data.rs:157-171): [2, 0x60, fmt, 0 x5, f64 fd, f64 f0].
+ * fmt is 0x24 (U8) for the u8 and u16 formats, as the reference writes, and
+ * 0x1C (F32le) for the f32 extension. */
+int sk_spectrum_topic(uint8_t out[24], int32_t spectrum_format, double fd, double f0);
+/* bytes_per_input_sample / is_input_format_complex (inputformats.rs:12-44);
+ * negative for an unknown format. */
+int sk_format_bytes(int32_t input_format);
+int sk_format_is_complex(int32_t input_format);
+
+const char* sk_last_error(void);
+const char* sk_version(void);
+
+/* ------------------------------------------------------------ plans
+ * DspState::init + Fcfb::add_filter per filter.  filter_status (optional,
+ * n_filters entries) receives SK_OK or the reason each filter was dropped. */
+int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_filters,
+                   int32_t* filter_status, sk_plan** out);
+int sk_plan_info_get(const sk_plan* plan, sk_plan_info* info);
+int sk_plan_channel(const sk_plan* plan, int32_t channel, sk_channel_info* info);
+void sk_plan_destroy(sk_plan* plan);
+
+/* Replace one channel's complex64 weights (natural order, `bins` values). */
+int sk_set_weights(sk_plan* plan, int32_t channel, const float* weights_c64);
+/* Copy one channel's current weights out (host memory). */
+int sk_get_weights(const sk_plan* plan, int32_t channel, float* weights_c64);
+
+/* One input buffer — DspState::process_real/process_complex with the
+ * reference main loop's overlap carry (main.rs:171-191).
+ *   raw        : info.raw_bytes of new samples in the plan's input format
+ *   chan_out[c]: channel c's B*3n/4 complex64 output samples (payload of its
+ *                record, fcfb.rs:84-87), c in [0, n_channels)
+ *   spec_out   : room for info.max_spectra * info.spectrum_bytes; receives the
+ *                payloads of the spectrum records completed by this call
+ * sk_process takes host pointers (copies in, computes, copies out, returns
+ * when done).  sk_process_device takes device pointers and only enqueues on
+ * `stream` (a cudaStream_t; NULL = the plan's own stream). */
+int sk_process(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out, sk_result* result);
+int sk_process_device(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out,
+                      sk_result* result, void* stream);
+/* Wait for all work the plan enqueued. */
+int sk_synchronize(sk_plan* plan);
+/* Number of device kernels one sk_process_device call launches. */
+int sk_launches_per_call(const sk_plan* plan);
+
+/* ------------------------------------------------------------ differentiable filter bank
+ * The filter-bank stage y_c = keep(IFFT_n(W'_c * gather(X, first_c))) as a
+ * separate forward / adjoint pair on device spectra, for gradient-based
+ * weight design.  X is [B][K] complex64 (the forward FFT of B blocks).
+ *   sk_spectra_device : raw -> X for one buffer (advances the halo and the
+ *                       Welch state exactly like sk_process_device)
+ *   sk_fcfb_forward_device : X, W -> y (W_dev[c] = complex64[n_c] natural order)
+ *   sk_fcfb_backward_device: X, W, dy -> dW (summed over blocks) and dX
+ *                       (accumulated into dX when not NULL); gradients follow
+ *                       torch's convention for real losses of complex tensors
+ *                       (dL/d conj(z)). */
+int sk_spectra_device(sk_plan* plan, const void* raw, float* X, void* stream);
+int sk_fcfb_forward_device(sk_plan* plan, const float* X, const float* const* W, float* const* y, void* stream);
+int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W, const float* const* dy,
+                            float* const* dW, float* dX, void* stream);
+
+/* Per-stage device timing with CUDA events recorded on the launching stream
+ * (off by default).  Stages: 0 forward FFT, 1 spectrum split + Welch terms,
+ * 2 Welch accumulation, 3 filter bank.  sk_plan_timing waits for the
+ * recorded work, returns the summed milliseconds per stage and the number of
+ * calls measured, and resets the totals. */
+#define SK_N_STAGES 4
+int sk_plan_set_timing(sk_plan* plan, int enable);
+int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
+
+/* Pinned host memory for staging (cudaHostAlloc); NULL on failure. */
+void* sk_host_alloc(size_t bytes);
+void sk_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPEKTRI_B200_H */

@@ -1,0 +1,715 @@
+// Plans and the device half of the C ABI (include/spektri_b200.h).
+//
+// A plan is DspState (dsp.rs:42-55) on one GPU: sizes from DspState::init
+// (dsp.rs:76-111), filters validated like Fcfb::add_filter (fcfb.rs:41-64),
+// and per call the stage order of process_real/process_complex
+// (dsp.rs:114-160): forward FFTs, Welch accumulation, filter bank.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "spektri_b200.h"
+#include "sk_internal.h"
+#include "sk_kernels.cuh"
+
+using namespace sk;
+
+namespace {
+
+constexpr int S = TILE_S;
+constexpr int T = TILE_T;
+constexpr size_t TILE_SMEM = TileShape<S>::SMEM_BYTES;
+
+int ilog2_exact(long long v) {
+  if (v <= 0 || (v & (v - 1))) return -1;
+  int r = 0;
+  while ((1ll << r) < v) ++r;
+  return r;
+}
+
+#define SK_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(SK_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// Scoped device selection (restores the caller's current device).
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+}  // namespace
+
+struct sk_plan {
+  sk_params p{};
+  int fmt = 0;
+  bool cplx = false;
+  long long N = 0, overlap = 0, hop = 0, nnew = 0, total = 0;
+  int K = 0, B = 0;
+  int log2N = 0, log2Nc = 0, R1 = 1, log2R1 = 0;
+  float wscale = 0.f;
+  int spec_fmt = 0, spec_bin_bytes = 1;
+  int averages = 1;
+  float db_plus = 0.f;
+  uint32_t accn = 0;
+  uint64_t spec_seq = 0;
+  int max_spectra = 1;
+  size_t raw_bytes = 0;
+
+  struct Chan {
+    uint32_t n = 0;
+    int log2n = 0;
+    long long first = 0;
+    double fs_out = 0, fc_out = 0;
+    int filter_index = 0;
+    size_t w_off = 0;     // complex offset into the weight buffer
+    size_t out_off = 0;   // complex offset into the plan's own output buffer
+  };
+  std::vector<Chan> ch;
+  std::vector<float> w_host;     // complex64, natural order, all channels
+
+  // device state
+  float2* d_tw_tile = nullptr;
+  float2* d_tw_big = nullptr;
+  float* d_halo[2] = {nullptr, nullptr};
+  int halo_cur = 0;
+  float2* d_Z = nullptr;
+  float2* d_X = nullptr;
+  float* d_P = nullptr;
+  float* d_acc = nullptr;
+  float2* d_w = nullptr;
+  ChanDev* d_chans = nullptr;
+  std::vector<ChanDev> h_chans;
+  std::vector<ChanDev> h_chans_uploaded;
+  ChanDev* d_chans_aux = nullptr;
+  BwdChan* d_bwd = nullptr;
+  TileDesc* d_tiles = nullptr;
+  int n_batched_tiles = 0;
+  std::vector<int> plain_start, plain_count;
+  int2* d_list = nullptr;
+  int* d_cursor = nullptr;
+  int persist_grid = 1;
+  cudaStream_t stream = nullptr;
+  // buffers of the host-pointer path
+  uint8_t* d_raw = nullptr;
+  float2* d_out = nullptr;
+  uint8_t* d_spec = nullptr;
+  size_t out_total = 0;
+  std::vector<void*> d_out_ptrs;
+  // stage timing
+  bool timing = false;
+  std::vector<std::array<cudaEvent_t, SK_N_STAGES + 1>> ev_pending, ev_free;
+  double stage_ms[SK_N_STAGES] = {0, 0, 0, 0};
+  uint64_t timed_calls = 0;
+};
+
+namespace {
+
+int plan_free(sk_plan* pl) {
+  if (!pl) return SK_OK;
+  DeviceGuard g(pl->p.device);
+  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_X, pl->d_P,
+                  pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->d_tiles, pl->d_list,
+                  pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
+  for (void* q : ptrs) if (q) cudaFree(q);
+  for (auto* v : {&pl->ev_pending, &pl->ev_free})
+    for (auto& a : *v)
+      for (auto e : a) cudaEventDestroy(e);
+  if (pl->stream) cudaStreamDestroy(pl->stream);
+  delete pl;
+  return SK_OK;
+}
+
+template <class TT>
+int dev_alloc(TT** p, size_t count) {
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, sizeof(TT) * count);
+  if (e != cudaSuccess) return fail(SK_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", sizeof(TT) * count, cudaGetErrorString(e));
+  return SK_OK;
+}
+
+void twiddles(std::vector<float2>& t, long long n) {
+  t.resize((size_t)n);
+  for (long long k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    t[(size_t)k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+}
+
+// Kernel instances per input format.
+using FwdFn = void (*)(FwdArgs);
+template <int FMT>
+FwdFn fwd_for() { return fwd_fft_kernel<S, T, FMT>; }
+FwdFn fwd_kernel_for(int fmt) {
+  switch (fmt) {
+    case SK_FMT_S8: return fwd_for<SK_FMT_S8>();
+    case SK_FMT_S16LE: return fwd_for<SK_FMT_S16LE>();
+    case SK_FMT_S16BE: return fwd_for<SK_FMT_S16BE>();
+    case SK_FMT_F32LE: return fwd_for<SK_FMT_F32LE>();
+    case SK_FMT_F32BE: return fwd_for<SK_FMT_F32BE>();
+    case SK_FMT_U8: return fwd_for<SK_FMT_U8>();
+    case SK_FMT_CS8: return fwd_for<SK_FMT_CS8>();
+    case SK_FMT_CS16LE: return fwd_for<SK_FMT_CS16LE>();
+    case SK_FMT_CS16BE: return fwd_for<SK_FMT_CS16BE>();
+    case SK_FMT_CF32LE: return fwd_for<SK_FMT_CF32LE>();
+    case SK_FMT_CF32BE: return fwd_for<SK_FMT_CF32BE>();
+    case SK_FMT_CU8: return fwd_for<SK_FMT_CU8>();
+  }
+  return nullptr;
+}
+
+int set_smem_attrs(FwdFn f) {
+  SK_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_backward_kernel<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  SK_CUDA(cudaFuncSetAttribute(fcfb_backward_kernel<S, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+  return SK_OK;
+}
+
+// Events for one timed call (recycled); nullptr when timing is off.
+std::array<cudaEvent_t, SK_N_STAGES + 1>* timing_events(sk_plan* pl) {
+  if (!pl->timing) return nullptr;
+  std::array<cudaEvent_t, SK_N_STAGES + 1> ev{};
+  if (!pl->ev_free.empty()) {
+    ev = pl->ev_free.back();
+    pl->ev_free.pop_back();
+  } else {
+    for (auto& e : ev)
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  }
+  pl->ev_pending.push_back(ev);
+  return &pl->ev_pending.back();
+}
+
+int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, float* P, cudaStream_t st,
+                   std::array<cudaEvent_t, SK_N_STAGES + 1>* ev = nullptr) {
+  FwdArgs a{};
+  a.raw = raw;
+  a.halo = pl->d_halo[pl->halo_cur];
+  a.halo_next = pl->d_halo[pl->halo_cur ^ 1];
+  a.overlap = pl->overlap;
+  a.nnew = pl->nnew;
+  a.hop = (int)pl->hop;
+  a.B = pl->B;
+  a.log2N = pl->log2N;
+  a.log2Nc = pl->log2Nc;
+  a.R1 = pl->R1;
+  a.log2R1 = pl->log2R1;
+  a.wscale = pl->wscale;
+  a.tw_tile = pl->d_tw_tile;
+  a.tw_big = pl->d_tw_big;
+  a.Z = pl->d_Z;
+  int grid;
+  if (pl->R1 == 1) {
+    const int per = S >> pl->log2Nc;
+    grid = (pl->B + per - 1) / per;
+  } else {
+    grid = pl->B * pl->R1;
+  }
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[0], st));
+  fwd_kernel_for(pl->fmt)<<<grid, T, TILE_SMEM, st>>>(a);
+  SK_CUDA(cudaGetLastError());
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[1], st));
+  SplitArgs s{};
+  s.Z = pl->d_Z;
+  s.X = X;
+  s.P = P;
+  s.log2N = pl->log2N;
+  s.log2Nc = pl->log2Nc;
+  s.K = pl->K;
+  s.R1 = pl->R1;
+  s.log2R1 = pl->log2R1;
+  s.logS = TileShape<S>::LOGS;
+  s.tw_big = pl->d_tw_big;
+  dim3 g2((pl->K + 255) / 256, pl->B);
+  if (pl->cplx) welch_split_kernel<false><<<g2, 256, 0, st>>>(s);
+  else welch_split_kernel<true><<<g2, 256, 0, st>>>(s);
+  SK_CUDA(cudaGetLastError());
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[2], st));
+  pl->halo_cur ^= 1;
+  return SK_OK;
+}
+
+FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
+  FcfbArgs a{};
+  a.tiles = pl->d_tiles;
+  a.ntiles = pl->n_batched_tiles;
+  a.cursor = pl->d_cursor;
+  a.list = pl->d_list;
+  a.chans = chans;
+  a.X = X;
+  a.K = pl->K;
+  a.log2N = pl->log2N;
+  a.tw = pl->d_tw_tile;
+  return a;
+}
+
+int launch_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
+  if (pl->ch.empty()) return SK_OK;
+  FcfbArgs a = fcfb_args(pl, chans, X);
+  if (batched) {
+    SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
+    const int grid = std::min(pl->persist_grid, pl->n_batched_tiles);
+    if (pl->cplx) fcfb_kernel<S, T, true, false><<<grid, T, TILE_SMEM, st>>>(a, 0);
+    else fcfb_kernel<S, T, true, true><<<grid, T, TILE_SMEM, st>>>(a, 0);
+    SK_CUDA(cudaGetLastError());
+  } else {
+    for (size_t c = 0; c < pl->ch.size(); ++c) {
+      if (pl->cplx) fcfb_kernel<S, T, false, false><<<pl->plain_count[c], T, TILE_SMEM, st>>>(a, pl->plain_start[c]);
+      else fcfb_kernel<S, T, false, true><<<pl->plain_count[c], T, TILE_SMEM, st>>>(a, pl->plain_start[c]);
+      SK_CUDA(cudaGetLastError());
+    }
+  }
+  return SK_OK;
+}
+
+int check_plan(const sk_plan* pl) {
+  if (!pl) return fail(SK_ERR_ARG, "null plan");
+  return SK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_filters, int32_t* filter_status,
+                   sk_plan** out) {
+  clear_error();
+  if (!params || !out || n_filters < 0 || (n_filters > 0 && !filters)) return fail(SK_ERR_ARG, "sk_plan_create: null argument");
+  *out = nullptr;
+  const sk_params& p = *params;
+  if (p.flags != 0) return fail(SK_ERR_ARG, "flags must be 0");
+  if (!format_valid(p.input_format)) return fail(SK_ERR_ARG, "unknown input format 0x%02x", p.input_format);
+  if (p.spectrum_format < SK_SPEC_U8 || p.spectrum_format > SK_SPEC_F32) return fail(SK_ERR_ARG, "unknown spectrum format %d", p.spectrum_format);
+  if (p.mode != SK_MODE_PLAIN && p.mode != SK_MODE_BATCHED) return fail(SK_ERR_ARG, "unknown mode %d", p.mode);
+  if (p.ffts_per_buf == 0) return fail(SK_ERR_ARG, "fftbuf must be positive");
+  const bool cplx = format_complex(p.input_format);
+  if (!cplx && (p.ffts_per_buf % 2)) return fail(SK_ERR_ARG, "fftbuf must be even for real input (blocks are transformed in pairs, multifft.rs:57-61)");
+  const int log2N = ilog2_exact(p.fft_size);
+  const int log2Nc = log2N - (cplx ? 0 : 1);
+  if (log2N < 0 || log2Nc < 2 || log2N < 3) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path needs a power of two >= 8", p.fft_size);
+  const int maxLogNc = TileShape<S>::LOGS + 3;   // R1 <= 8
+  if (log2Nc > maxLogNc) return fail(SK_ERR_UNSUPPORTED, "FFT size %u exceeds the device limit (complex length %d)", p.fft_size, 1 << maxLogNc);
+
+  sk_plan* pl = new sk_plan();
+  pl->p = p;
+  pl->fmt = p.input_format;
+  pl->cplx = cplx;
+  pl->N = p.fft_size;
+  pl->overlap = pl->N / 4;                 // dsp.rs:77
+  pl->hop = pl->N - pl->overlap;           // dsp.rs:78
+  pl->B = (int)p.ffts_per_buf;
+  pl->nnew = pl->hop * pl->B;              // dsp.rs:107-110
+  pl->total = pl->nnew + pl->overlap;
+  pl->K = cplx ? (int)pl->N : (int)(pl->N / 2 + 1);
+  pl->log2N = log2N;
+  pl->log2Nc = log2Nc;
+  if (log2Nc > TileShape<S>::LOGS) {
+    pl->log2R1 = log2Nc - TileShape<S>::LOGS;
+    pl->R1 = 1 << pl->log2R1;
+  }
+  pl->wscale = format_scaling(p.input_format) / (float)pl->N;      // dsp.rs:70-73
+  pl->spec_fmt = p.spectrum_format;
+  pl->spec_bin_bytes = p.spectrum_format == SK_SPEC_U8 ? 1 : p.spectrum_format == SK_SPEC_U16 ? 2 : 4;
+  pl->averages = (int)std::max<uint32_t>(1, p.averages);           // averages 0 behaves as 1 (accn >= averages)
+  pl->db_plus = std::log10((float)pl->averages) * -10.0f;          // spectrum.rs:130
+  pl->max_spectra = (pl->B + pl->averages - 1) / pl->averages + 1;
+  pl->raw_bytes = (size_t)pl->nnew * format_bytes(pl->fmt);
+
+  // Filters (fcfb.rs:41-64): inexact parameters are dropped.
+  int dropped = 0;
+  for (int i = 0; i < n_filters; ++i) {
+    long long bins = 0, first = 0;
+    int st = SK_OK;
+    if (!freq_to_bins_exact(p.fs_in, p.fc_in, pl->N, filters[i].fs_out, filters[i].fc_out, &bins, &first)) {
+      st = SK_ERR_FILTER;
+      fprintf(stderr, "Invalid filter parameters\n");
+    } else {
+      const int l2 = ilog2_exact(bins);
+      if (l2 < 2 || l2 > TileShape<S>::LOGS) {
+        st = SK_ERR_UNSUPPORTED;
+        fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two 4..%d)\n", bins, S);
+      } else {
+        sk_plan::Chan c;
+        c.n = (uint32_t)bins;
+        c.log2n = l2;
+        c.first = first;
+        c.fs_out = filters[i].fs_out;
+        c.fc_out = filters[i].fc_out;
+        c.filter_index = i;
+        c.w_off = pl->w_host.size() / 2;
+        pl->w_host.resize(pl->w_host.size() + 2 * (size_t)bins);
+        float* w = pl->w_host.data() + 2 * c.w_off;
+        if (filters[i].weights) std::memcpy(w, filters[i].weights, sizeof(float) * 2 * bins);
+        else if (filters[i].transition > 0) tukey((uint32_t)bins, filters[i].transition, w);
+        else raised_cosine((uint32_t)bins, w);
+        pl->ch.push_back(c);
+      }
+    }
+    if (st != SK_OK) ++dropped;
+    if (filter_status) filter_status[i] = st;
+  }
+  size_t off = 0;
+  for (auto& c : pl->ch) { c.out_off = off; off += (size_t)pl->B * (c.n / 8 * 6); }
+  pl->out_total = off;
+
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+    plan_free(pl);
+    return fail(SK_ERR_CUDA, "no CUDA device available");
+  }
+  if (p.device < 0 || p.device >= dev_count) { plan_free(pl); return fail(SK_ERR_ARG, "device %d out of range", p.device); }
+  DeviceGuard g(p.device);
+  if (!g.ok) { plan_free(pl); return fail(SK_ERR_CUDA, "cudaSetDevice(%d) failed", p.device); }
+  int rc = SK_OK;
+#define TRY(x) do { rc = (x); if (rc != SK_OK) { plan_free(pl); return rc; } } while (0)
+  TRY(set_smem_attrs(fwd_kernel_for(pl->fmt)));
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { plan_free(pl); return fail(SK_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
+  }
+  std::vector<float2> tws, twb;
+  twiddles(tws, S);
+  twiddles(twb, pl->N);
+  TRY(dev_alloc(&pl->d_tw_tile, tws.size()));
+  TRY(dev_alloc(&pl->d_tw_big, twb.size()));
+  const size_t halo_n = (size_t)pl->overlap * (cplx ? 2 : 1);
+  TRY(dev_alloc(&pl->d_halo[0], halo_n));
+  TRY(dev_alloc(&pl->d_halo[1], halo_n));
+  TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
+  TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->K));
+  TRY(dev_alloc(&pl->d_P, (size_t)pl->B * pl->K));
+  TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
+  TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
+  TRY(dev_alloc(&pl->d_chans, pl->ch.size()));
+  TRY(dev_alloc(&pl->d_chans_aux, pl->ch.size()));
+  TRY(dev_alloc(&pl->d_bwd, pl->ch.size()));
+  TRY(dev_alloc(&pl->d_cursor, 1));
+  TRY(dev_alloc(&pl->d_raw, pl->raw_bytes));
+  TRY(dev_alloc(&pl->d_out, pl->out_total));
+  TRY(dev_alloc(&pl->d_spec, (size_t)pl->max_spectra * pl->K * pl->spec_bin_bytes));
+#define CUDA_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { plan_free(pl); return fail(SK_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); } } while (0)
+  CUDA_TRY(cudaMemcpy(pl->d_tw_tile, tws.data(), sizeof(float2) * tws.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(pl->d_tw_big, twb.data(), sizeof(float2) * twb.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemset(pl->d_halo[0], 0, sizeof(float) * std::max<size_t>(1, halo_n)));   // main.rs:165: zeros
+  CUDA_TRY(cudaMemset(pl->d_halo[1], 0, sizeof(float) * std::max<size_t>(1, halo_n)));
+  CUDA_TRY(cudaMemset(pl->d_acc, 0, sizeof(float) * pl->K));
+  if (!pl->w_host.empty())
+    CUDA_TRY(cudaMemcpy(pl->d_w, pl->w_host.data(), sizeof(float) * pl->w_host.size(), cudaMemcpyHostToDevice));
+
+  // Channel table (output pointers start at the plan's own buffer).
+  pl->h_chans.resize(pl->ch.size());
+  for (size_t c = 0; c < pl->ch.size(); ++c) {
+    ChanDev d{};
+    d.w = pl->d_w + pl->ch[c].w_off;
+    d.out = pl->d_out + pl->ch[c].out_off;
+    d.first = pl->ch[c].first;
+    d.log2n = pl->ch[c].log2n;
+    pl->h_chans[c] = d;
+    pl->d_out_ptrs.push_back(d.out);
+  }
+  if (!pl->h_chans.empty())
+    CUDA_TRY(cudaMemcpy(pl->d_chans, pl->h_chans.data(), sizeof(ChanDev) * pl->h_chans.size(), cudaMemcpyHostToDevice));
+  pl->h_chans_uploaded = pl->h_chans;
+
+  // Work lists.  Batched: channels grouped by IFFT size, largest first, each
+  // size's (channel, block) transforms packed S/n to a tile.  Plain: each
+  // channel's own tiles.
+  std::vector<int2> list;
+  std::vector<TileDesc> tiles;
+  for (int l2 = TileShape<S>::LOGS; l2 >= 2; --l2) {
+    const int per = S >> l2;
+    const int base = (int)list.size();
+    for (size_t c = 0; c < pl->ch.size(); ++c)
+      if (pl->ch[c].log2n == l2)
+        for (int b = 0; b < pl->B; ++b) list.push_back(make_int2((int)c, b));
+    const int cnt = (int)list.size() - base;
+    for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
+  }
+  pl->n_batched_tiles = (int)tiles.size();
+  for (size_t c = 0; c < pl->ch.size(); ++c) {
+    const int l2 = pl->ch[c].log2n, per = S >> l2;
+    const int base = (int)list.size();
+    for (int b = 0; b < pl->B; ++b) list.push_back(make_int2((int)c, b));
+    pl->plain_start.push_back((int)tiles.size());
+    for (int o = 0; o < pl->B; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, pl->B - o), 0});
+    pl->plain_count.push_back((int)tiles.size() - pl->plain_start.back());
+  }
+  TRY(dev_alloc(&pl->d_list, list.size()));
+  TRY(dev_alloc(&pl->d_tiles, tiles.size()));
+  if (!list.empty()) CUDA_TRY(cudaMemcpy(pl->d_list, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice));
+  if (!tiles.empty()) CUDA_TRY(cudaMemcpy(pl->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
+  int sms = 0, per_sm = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcfb_kernel<S, T, true, true>, T, TILE_SMEM));
+  pl->persist_grid = std::max(1, sms * std::max(1, per_sm));
+#undef TRY
+#undef CUDA_TRY
+  *out = pl;
+  return dropped ? SK_WARN_FILTER : SK_OK;
+}
+
+void sk_plan_destroy(sk_plan* pl) {
+  if (!pl) return;
+  {
+    DeviceGuard g(pl->p.device);
+    if (pl->stream) cudaStreamSynchronize(pl->stream);
+  }
+  plan_free(pl);
+}
+
+int sk_plan_info_get(const sk_plan* pl, sk_plan_info* info) {
+  if (check_plan(pl) || !info) return fail(SK_ERR_ARG, "null argument");
+  info->new_samples = (uint64_t)pl->nnew;
+  info->overlap = (uint64_t)pl->overlap;
+  info->total = (uint64_t)pl->total;
+  info->raw_bytes = pl->raw_bytes;
+  info->result_bins = (uint32_t)pl->K;
+  info->n_channels = (uint32_t)pl->ch.size();
+  info->max_spectra = (uint32_t)pl->max_spectra;
+  info->spectrum_bytes = (uint32_t)(pl->K * pl->spec_bin_bytes);
+  return SK_OK;
+}
+
+int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
+  if (check_plan(pl) || !info) return fail(SK_ERR_ARG, "null argument");
+  if (c < 0 || c >= (int)pl->ch.size()) return fail(SK_ERR_ARG, "channel %d out of range", c);
+  const auto& k = pl->ch[c];
+  info->bins = k.n;
+  info->filter_index = k.filter_index;
+  info->first = k.first;
+  info->fs_out = k.fs_out;
+  info->fc_out = k.fc_out;
+  info->out_samples = (uint64_t)pl->B * (k.n / 8 * 6);
+  return SK_OK;
+}
+
+int sk_launches_per_call(const sk_plan* pl) {
+  if (!pl) return fail(SK_ERR_ARG, "null plan");
+  const int fb = pl->ch.empty() ? 0 : (pl->p.mode == SK_MODE_BATCHED ? 1 : (int)pl->ch.size());
+  return 3 + fb;
+}
+
+int sk_set_weights(sk_plan* pl, int32_t c, const float* w) {
+  if (check_plan(pl) || !w) return fail(SK_ERR_ARG, "null argument");
+  if (c < 0 || c >= (int)pl->ch.size()) return fail(SK_ERR_ARG, "channel %d out of range", c);
+  DeviceGuard g(pl->p.device);
+  const auto& k = pl->ch[c];
+  std::memcpy(pl->w_host.data() + 2 * k.w_off, w, sizeof(float) * 2 * k.n);
+  // Ordered after earlier work on the plan's stream.
+  SK_CUDA(cudaStreamSynchronize(pl->stream));
+  SK_CUDA(cudaMemcpy(pl->d_w + k.w_off, w, sizeof(float2) * k.n, cudaMemcpyHostToDevice));
+  return SK_OK;
+}
+
+int sk_get_weights(const sk_plan* pl, int32_t c, float* w) {
+  if (check_plan(pl) || !w) return fail(SK_ERR_ARG, "null argument");
+  if (c < 0 || c >= (int)pl->ch.size()) return fail(SK_ERR_ARG, "channel %d out of range", c);
+  const auto& k = pl->ch[c];
+  std::memcpy(w, pl->w_host.data() + 2 * k.w_off, sizeof(float) * 2 * k.n);
+  return SK_OK;
+}
+
+int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_out, sk_result* result,
+                      void* stream) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!raw) return fail(SK_ERR_ARG, "null raw input");
+  if (!pl->ch.empty() && !chan_out) return fail(SK_ERR_ARG, "null channel output table");
+  const int align = format_bits(pl->fmt) / 8;
+  if ((uintptr_t)raw % align) return fail(SK_ERR_ARG, "raw input must be %d-byte aligned", align);
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  // Channel output pointers (re-uploaded only when they change).
+  bool changed = false;
+  for (size_t c = 0; c < pl->ch.size(); ++c) {
+    if (!chan_out[c]) return fail(SK_ERR_ARG, "null output for channel %zu", c);
+    if ((uintptr_t)chan_out[c] % 8) return fail(SK_ERR_ARG, "channel %zu output must be 8-byte aligned", c);
+    pl->h_chans[c].out = (float2*)chan_out[c];
+    if (pl->h_chans[c].out != pl->h_chans_uploaded[c].out) changed = true;
+  }
+  if (changed) {
+    SK_CUDA(cudaMemcpyAsync(pl->d_chans, pl->h_chans.data(), sizeof(ChanDev) * pl->h_chans.size(), cudaMemcpyHostToDevice, st));
+    SK_CUDA(cudaStreamSynchronize(st));   // the host table may change again next call
+    pl->h_chans_uploaded = pl->h_chans;
+  }
+  // Spectrum bookkeeping (spectrum.rs:112-161): records complete every `averages` blocks.
+  const uint32_t total = pl->accn + (uint32_t)pl->B;
+  const uint32_t n_spec = total / (uint32_t)pl->averages;
+  if (n_spec > 0 && !spec_out) return fail(SK_ERR_ARG, "spectrum records complete in this call but spec_out is null");
+  auto* ev = timing_events(pl);
+  int rc = launch_forward(pl, (const uint8_t*)raw, pl->d_X, pl->d_P, st, ev);
+  if (rc) return rc;
+  welch_accum_kernel<<<(pl->K + 255) / 256, 256, 0, st>>>(pl->d_P, pl->d_acc, pl->K, pl->B, (int)pl->accn,
+                                                          pl->averages, pl->spec_fmt, pl->db_plus, (uint8_t*)spec_out);
+  SK_CUDA(cudaGetLastError());
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[3], st));
+  rc = launch_fcfb(pl, pl->d_chans, pl->d_X, pl->p.mode == SK_MODE_BATCHED, st);
+  if (rc) return rc;
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[4], st));
+  if (result) {
+    result->n_spectra = n_spec;
+    result->reserved = 0;
+    result->spectrum_seq0 = pl->spec_seq;
+  }
+  pl->accn = total % (uint32_t)pl->averages;
+  pl->spec_seq += n_spec;
+  return SK_OK;
+}
+
+int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_out, sk_result* result) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!raw) return fail(SK_ERR_ARG, "null raw input");
+  if (!pl->ch.empty() && !chan_out) return fail(SK_ERR_ARG, "null channel output table");
+  for (size_t c = 0; c < pl->ch.size(); ++c)
+    if (!chan_out[c]) return fail(SK_ERR_ARG, "null output for channel %zu", c);
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = pl->stream;
+  SK_CUDA(cudaMemcpyAsync(pl->d_raw, raw, pl->raw_bytes, cudaMemcpyHostToDevice, st));
+  sk_result r{};
+  const uint32_t n_spec_expected = (pl->accn + (uint32_t)pl->B) / (uint32_t)pl->averages;
+  if (n_spec_expected > 0 && !spec_out) return fail(SK_ERR_ARG, "spectrum records complete in this call but spec_out is null");
+  int rc = sk_process_device(pl, pl->d_raw, pl->d_out_ptrs.data(), pl->d_spec, &r, st);
+  if (rc) return rc;
+  for (size_t c = 0; c < pl->ch.size(); ++c) {
+    const size_t bytes = sizeof(float2) * (size_t)pl->B * (pl->ch[c].n / 8 * 6);
+    SK_CUDA(cudaMemcpyAsync(chan_out[c], pl->d_out + pl->ch[c].out_off, bytes, cudaMemcpyDeviceToHost, st));
+  }
+  if (r.n_spectra)
+    SK_CUDA(cudaMemcpyAsync(spec_out, pl->d_spec, (size_t)r.n_spectra * pl->K * pl->spec_bin_bytes, cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  if (result) *result = r;
+  return SK_OK;
+}
+
+int sk_synchronize(sk_plan* pl) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  DeviceGuard g(pl->p.device);
+  SK_CUDA(cudaStreamSynchronize(pl->stream));
+  SK_CUDA(cudaDeviceSynchronize());
+  return SK_OK;
+}
+
+int sk_spectra_device(sk_plan* pl, const void* raw, float* X, void* stream) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!raw || !X) return fail(SK_ERR_ARG, "null argument");
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  return launch_forward(pl, (const uint8_t*)raw, (float2*)X, nullptr, st);
+}
+
+int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, float* const* y, void* stream) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!X || (!pl->ch.empty() && (!W || !y))) return fail(SK_ERR_ARG, "null argument");
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  std::vector<ChanDev> aux(pl->h_chans);
+  for (size_t c = 0; c < aux.size(); ++c) {
+    if (!W[c] || !y[c]) return fail(SK_ERR_ARG, "null pointer for channel %zu", c);
+    aux[c].w = (const float2*)W[c];
+    aux[c].out = (float2*)y[c];
+  }
+  if (!aux.empty()) {
+    SK_CUDA(cudaMemcpyAsync(pl->d_chans_aux, aux.data(), sizeof(ChanDev) * aux.size(), cudaMemcpyHostToDevice, st));
+    SK_CUDA(cudaStreamSynchronize(st));
+  }
+  if (pl->ch.empty()) return SK_OK;
+  FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
+  if (pl->cplx) fcfb_kernel<S, T, false, false><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a, 0);
+  else fcfb_kernel<S, T, false, true><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a, 0);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, const float* const* dy,
+                            float* const* dW, float* dX, void* stream) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!X || (!pl->ch.empty() && (!W || !dy || !dW))) return fail(SK_ERR_ARG, "null argument");
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  std::vector<BwdChan> bc(pl->ch.size());
+  for (size_t c = 0; c < bc.size(); ++c) {
+    if (!W[c] || !dy[c] || !dW[c]) return fail(SK_ERR_ARG, "null pointer for channel %zu", c);
+    bc[c].w = (const float2*)W[c];
+    bc[c].dy = (const float2*)dy[c];
+    bc[c].dw = (float2*)dW[c];
+    bc[c].first = pl->ch[c].first;
+    bc[c].log2n = pl->ch[c].log2n;
+    SK_CUDA(cudaMemsetAsync(dW[c], 0, sizeof(float2) * pl->ch[c].n, st));
+  }
+  if (bc.empty()) return SK_OK;
+  SK_CUDA(cudaMemcpyAsync(pl->d_bwd, bc.data(), sizeof(BwdChan) * bc.size(), cudaMemcpyHostToDevice, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  BwdArgs a{};
+  a.tiles = pl->d_tiles;
+  a.list = pl->d_list;
+  a.chans = pl->d_bwd;
+  a.X = (const float2*)X;
+  a.dX = (float2*)dX;
+  a.K = pl->K;
+  a.log2N = pl->log2N;
+  a.tw = pl->d_tw_tile;
+  if (pl->cplx) fcfb_backward_kernel<S, T, false><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a);
+  else fcfb_backward_kernel<S, T, true><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+int sk_plan_set_timing(sk_plan* pl, int enable) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  pl->timing = enable != 0;
+  return SK_OK;
+}
+
+int sk_plan_timing(sk_plan* pl, double* ms, uint64_t* calls) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  DeviceGuard g(pl->p.device);
+  for (auto& ev : pl->ev_pending) {
+    SK_CUDA(cudaEventSynchronize(ev[SK_N_STAGES]));
+    for (int s = 0; s < SK_N_STAGES; ++s) {
+      float t = 0.f;
+      SK_CUDA(cudaEventElapsedTime(&t, ev[s], ev[s + 1]));
+      pl->stage_ms[s] += t;
+    }
+    pl->timed_calls += 1;
+    pl->ev_free.push_back(ev);
+  }
+  pl->ev_pending.clear();
+  for (int s = 0; s < SK_N_STAGES; ++s) {
+    if (ms) ms[s] = pl->stage_ms[s];
+    pl->stage_ms[s] = 0;
+  }
+  if (calls) *calls = pl->timed_calls;
+  pl->timed_calls = 0;
+  return SK_OK;
+}
+
+void* sk_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocPortable) != cudaSuccess) {
+    fail(SK_ERR_NOMEM, "cudaHostAlloc(%zu) failed", bytes);
+    return nullptr;
+  }
+  return p;
+}
+
+void sk_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

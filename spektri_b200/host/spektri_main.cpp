@@ -1,0 +1,284 @@
+// spektri — drop-in replacement for the reference binary (spektri/src/main.rs)
+// with the filter bank and spectrum on a B200 through libspektri_b200.
+//
+// Same command line (main.rs:15-66), filter grammar (main.rs:70-91), stdin
+// framing (main.rs:113-193) and outputs: every record is published on a
+// ZeroMQ PUB socket as (topic24, metadata24 + payload) (output.rs:49-60),
+// filter records are appended to their file= (header + payload), spectrum
+// records are also written to stdout (spectrum.rs:73-78).  Per buffer the
+// spectrum records come first, then the filters in their configured order
+// (dsp.rs:157-158, fcfb.rs:93-95).
+//
+// Additions, all off by default: --spectrumformat=f32, filter keys tw= and w=,
+// --mode=plain|batched (default batched), --device=N and
+// --fake-clock=<secs>,<step_ns> (deterministic timestamps for tests).
+#include <cerrno>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <strings.h>
+#include <unistd.h>
+#include <vector>
+
+#include "spektri_b200.h"
+#include "zmq_pub.h"
+
+namespace {
+
+struct FilterArg {
+  double fs = 0, fc = 0;
+  std::string file, wpath;
+  uint32_t tw = 0;
+  std::vector<float> weights;
+};
+
+[[noreturn]] void usage_error(const std::string& msg) {
+  fprintf(stderr, "error: %s\n", msg.c_str());
+  exit(1);   // clap's Error::exit
+}
+
+[[noreturn]] void panic(const std::string& msg) {
+  fprintf(stderr, "thread 'main' panicked: %s\n", msg.c_str());
+  exit(101); // Rust panic exit code
+}
+
+int parse_format(const std::string& s) {
+  static const struct { const char* n; int c; } t[] = {
+      {"s8", SK_FMT_S8}, {"s16le", SK_FMT_S16LE}, {"s16be", SK_FMT_S16BE}, {"f32le", SK_FMT_F32LE},
+      {"f32be", SK_FMT_F32BE}, {"u8", SK_FMT_U8}, {"cs8", SK_FMT_CS8}, {"cs16le", SK_FMT_CS16LE},
+      {"cs16be", SK_FMT_CS16BE}, {"cf32le", SK_FMT_CF32LE}, {"cf32be", SK_FMT_CF32BE}, {"cu8", SK_FMT_CU8}};
+  for (auto& e : t)
+    if (strcasecmp(s.c_str(), e.n) == 0) return e.c;
+  return -1;
+}
+
+double parse_f64(const std::string& v, const char* what, bool is_panic) {
+  char* end = nullptr;
+  errno = 0;
+  double d = strtod(v.c_str(), &end);
+  if (v.empty() || *end != 0) {
+    std::string m = std::string("invalid value '") + v + "' for " + what;
+    if (is_panic) panic(m);
+    usage_error(m);
+  }
+  return d;
+}
+
+long long parse_int(const std::string& v, const char* what) {
+  char* end = nullptr;
+  long long d = strtoll(v.c_str(), &end, 10);
+  if (v.empty() || *end != 0 || d < 0) usage_error(std::string("invalid value '") + v + "' for " + what);
+  return d;
+}
+
+// main.rs:70-91
+FilterArg parse_filter(const std::string& s) {
+  FilterArg f;
+  bool have_fs = false, have_fc = false;
+  size_t pos = 0;
+  while (true) {
+    size_t e = s.find(':', pos);
+    std::string kv = s.substr(pos, e == std::string::npos ? std::string::npos : e - pos);
+    size_t eq = kv.find('=');
+    if (eq == std::string::npos) panic("called `Option::unwrap()` on a `None` value (filter parameter '" + kv + "')");
+    std::string k = kv.substr(0, eq), v = kv.substr(eq + 1);
+    if (k == "fs") { f.fs = parse_f64(v, "fs", true); have_fs = true; }
+    else if (k == "fc") { f.fc = parse_f64(v, "fc", true); have_fc = true; }
+    else if (k == "file") f.file = v;
+    else if (k == "tw") f.tw = (uint32_t)parse_f64(v, "tw", true);
+    else if (k == "w") f.wpath = v;
+    if (e == std::string::npos) break;
+    pos = e + 1;
+  }
+  if (!have_fs || !have_fc) panic("called `Option::unwrap()` on a `None` value (filter needs fs= and fc=)");
+  if (!f.wpath.empty()) {
+    FILE* wf = fopen(f.wpath.c_str(), "rb");
+    if (!wf) panic("cannot read weights file " + f.wpath);
+    float buf[4096];
+    size_t r;
+    while ((r = fread(buf, sizeof(float), 4096, wf)) > 0) f.weights.insert(f.weights.end(), buf, buf + r);
+    fclose(wf);
+  }
+  return f;
+}
+
+bool read_exact(uint8_t* p, size_t n) {
+  size_t got = 0;
+  while (got < n) {
+    ssize_t r = read(0, p + got, n - got);
+    if (r < 0 && errno == EINTR) continue;
+    if (r <= 0) return false;
+    got += (size_t)r;
+  }
+  return true;
+}
+
+void write_all(FILE* f, const void* p, size_t n) {
+  if (f && n) fwrite(p, 1, n, f);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  sk_params p{};
+  p.fc_in = 0;
+  p.fft_size = 16384;         // main.rs:44
+  p.ffts_per_buf = 8;         // main.rs:49
+  p.averages = 2000;          // main.rs:55
+  p.spectrum_format = SK_SPEC_U8;
+  p.mode = SK_MODE_BATCHED;
+  p.device = 0;
+  bool have_fs = false;
+  int fmt = -1;
+  std::vector<std::string> filter_strs, binds;
+  bool fake = false;
+  unsigned long long clk_secs = 0, clk_step = 0;
+
+  auto take = [&](int& i, const std::string& a, const char* lng, const char* sht, std::string& out) -> bool {
+    const std::string L = std::string("--") + lng;
+    if (a == L || (sht && a == std::string("-") + sht)) {
+      if (i + 1 >= argc) usage_error("The argument '" + L + "' requires a value but none was supplied");
+      out = argv[++i];
+      return true;
+    }
+    if (a.rfind(L + "=", 0) == 0) { out = a.substr(L.size() + 1); return true; }
+    if (sht && a.size() > 2 && a.rfind(std::string("-") + sht, 0) == 0) {
+      out = a.substr(2);
+      if (!out.empty() && out[0] == '=') out = out.substr(1);
+      return true;
+    }
+    return false;
+  };
+  auto more_values = [&](int& i, std::vector<std::string>& dst) {
+    while (i + 1 < argc && argv[i + 1][0] != '-') dst.push_back(argv[++i]);
+  };
+  for (int i = 1; i < argc; ++i) {
+    std::string a = argv[i], v;
+    if (take(i, a, "samplerate", "s", v)) { p.fs_in = parse_f64(v, "samplerate", false); have_fs = true; }
+    else if (take(i, a, "centerfreq", "f", v)) p.fc_in = parse_f64(v, "centerfreq", false);
+    else if (take(i, a, "fftsize", "n", v)) p.fft_size = (uint32_t)parse_int(v, "fftsize");
+    else if (take(i, a, "fftbuf", nullptr, v)) p.ffts_per_buf = (uint32_t)parse_int(v, "fftbuf");
+    else if (take(i, a, "averages", "a", v)) p.averages = (uint32_t)parse_int(v, "averages");
+    else if (take(i, a, "inputformat", "I", v)) {
+      fmt = parse_format(v);
+      if (fmt < 0) usage_error("'" + v + "' isn't a valid value for '--inputformat <FORMAT>'");
+    } else if (take(i, a, "spectrumformat", nullptr, v)) {
+      if (strcasecmp(v.c_str(), "u8") == 0) p.spectrum_format = SK_SPEC_U8;
+      else if (strcasecmp(v.c_str(), "u16") == 0) p.spectrum_format = SK_SPEC_U16;
+      else if (strcasecmp(v.c_str(), "f32") == 0) p.spectrum_format = SK_SPEC_F32;
+      else usage_error("'" + v + "' isn't a valid value for '--spectrumformat <FORMAT>'");
+    } else if (take(i, a, "filters", nullptr, v)) { filter_strs.push_back(v); more_values(i, filter_strs); }
+    else if (take(i, a, "zmqbind", nullptr, v)) { binds.push_back(v); more_values(i, binds); }
+    else if (take(i, a, "mode", nullptr, v)) p.mode = (v == "plain") ? SK_MODE_PLAIN : SK_MODE_BATCHED;
+    else if (take(i, a, "device", nullptr, v)) p.device = (int32_t)parse_int(v, "device");
+    else if (take(i, a, "fake-clock", nullptr, v)) {
+      fake = true;
+      if (sscanf(v.c_str(), "%llu,%llu", &clk_secs, &clk_step) != 2) usage_error("--fake-clock=<secs>,<step_ns>");
+    } else usage_error("Found argument '" + a + "' which wasn't expected");
+  }
+  if (!have_fs) usage_error("The argument '--samplerate <HZ>' is required");
+  if (fmt < 0) usage_error("The argument '--inputformat <FORMAT>' is required");
+  p.input_format = fmt;
+  if (binds.empty()) binds.push_back("ipc:///tmp/spektri.zmq");   // main.rs:65
+
+  std::vector<FilterArg> fa;
+  for (auto& s : filter_strs) fa.push_back(parse_filter(s));
+
+  // main.rs:97-102
+  ZmqPub zmq;
+  std::string err;
+  if (!zmq.load(&err)) panic(err);
+  for (auto& b : binds)
+    if (!zmq.bind(b, &err)) panic(err);
+
+  std::vector<sk_filter> sf(fa.size());
+  for (size_t i = 0; i < fa.size(); ++i) {
+    sf[i].fs_out = fa[i].fs;
+    sf[i].fc_out = fa[i].fc;
+    sf[i].transition = fa[i].tw;
+    sf[i].weights = fa[i].weights.empty() ? nullptr : fa[i].weights.data();
+  }
+  std::vector<int32_t> status(fa.size(), 0);
+  sk_plan* plan = nullptr;
+  int rc = sk_plan_create(&p, sf.data(), (int32_t)sf.size(), status.data(), &plan);
+  if (rc < 0) {
+    fprintf(stderr, "spektri: %s\n", sk_last_error());
+    return rc == SK_ERR_ARG ? 101 : 1;
+  }
+  sk_plan_info info{};
+  sk_plan_info_get(plan, &info);
+
+  // One output per surviving filter (output.rs:24-46: a file that cannot be
+  // created only prints a message).
+  struct Out { uint8_t topic[24]; FILE* file = nullptr; uint64_t n = 0; };
+  std::vector<Out> outs(info.n_channels);
+  for (uint32_t c = 0; c < info.n_channels; ++c) {
+    sk_channel_info ci{};
+    sk_plan_channel(plan, (int32_t)c, &ci);
+    const FilterArg& f = fa[ci.filter_index];
+    sk_signal_topic(outs[c].topic, f.fs, f.fc);
+    outs[c].n = ci.out_samples;
+    if (!f.file.empty()) {
+      outs[c].file = fopen(f.file.c_str(), "wb");
+      if (!outs[c].file) fprintf(stderr, "Could not create file: %s\n", strerror(errno));
+    }
+  }
+  uint8_t spec_topic[24];
+  sk_spectrum_topic(spec_topic, p.spectrum_format, p.fs_in / (double)p.fft_size, p.fc_in);   // spectrum.rs:57-65
+
+  // Pinned staging: raw input, one record buffer per channel (24-byte header
+  // then payload), spectrum payloads.
+  const int bps = sk_format_bytes(fmt);
+  uint8_t* raw = (uint8_t*)sk_host_alloc(info.new_samples * (size_t)bps);
+  std::vector<uint8_t*> rec(info.n_channels);
+  std::vector<void*> payload(info.n_channels);
+  for (uint32_t c = 0; c < info.n_channels; ++c) {
+    rec[c] = (uint8_t*)sk_host_alloc(32 + outs[c].n * 8);
+    payload[c] = rec[c] + 32;   // 16-byte aligned payload; the header goes at +8
+  }
+  uint8_t* spec = (uint8_t*)sk_host_alloc((size_t)info.max_spectra * info.spectrum_bytes);
+  std::vector<uint8_t> srec(24 + info.spectrum_bytes);
+  if (!raw || !spec) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
+
+  uint64_t seq = 0;
+  const size_t raw_bytes = info.new_samples * (size_t)bps;
+  while (read_exact(raw, raw_bytes)) {        // main.rs:176-178: a short read ends the stream
+    uint64_t secs = 0;
+    uint32_t nanos = 0;
+    if (fake) {
+      const unsigned long long t = clk_secs * 1000000000ull + seq * clk_step;
+      secs = t / 1000000000ull;
+      nanos = (uint32_t)(t % 1000000000ull);
+    } else {
+      timespec ts;
+      clock_gettime(CLOCK_REALTIME, &ts);   // main.rs:180
+      secs = (uint64_t)ts.tv_sec;
+      nanos = (uint32_t)ts.tv_nsec;
+    }
+    sk_result r{};
+    rc = sk_process(plan, raw, payload.data(), spec, &r);
+    if (rc < 0) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
+    for (uint32_t s = 0; s < r.n_spectra; ++s) {
+      sk_serialize_metadata(srec.data(), r.spectrum_seq0 + s, secs, nanos);
+      std::memcpy(srec.data() + 24, spec + (size_t)s * info.spectrum_bytes, info.spectrum_bytes);
+      zmq.send2(spec_topic, 24, srec.data(), srec.size());
+      write_all(stdout, srec.data(), srec.size());
+    }
+    for (uint32_t c = 0; c < info.n_channels; ++c) {
+      uint8_t* h = rec[c] + 8;
+      sk_serialize_metadata(h, seq, secs, nanos);     // fcfb.rs:84: seq of the buffer
+      const size_t len = 24 + outs[c].n * 8;
+      zmq.send2(outs[c].topic, 24, h, len);
+      write_all(outs[c].file, h, len);
+    }
+    ++seq;
+  }
+  fflush(stdout);
+  for (auto& o : outs)
+    if (o.file) fclose(o.file);
+  sk_plan_destroy(plan);
+  return 0;
+}

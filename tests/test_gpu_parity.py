@@ -1,0 +1,212 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Bars: relative RMS <= 1e-5 against the FP64 oracle for channel outputs and
+f32 spectra; u8/u16 spectrum codes within 1 LSB; bin indices, record counts,
+sequence numbers and sample counts exact.  Plain and batched execution must
+agree bit for bit (same kernels, different scheduling).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from oracle import oracle32, oracle64
+from oracle.oracle64 import rel_rms
+from spektri_b200 import Plan, workloads
+from spektri_b200._lib import SK_ERR_FILTER, SK_ERR_UNSUPPORTED, SpektriError
+
+TOL = 1e-5
+
+
+def _o64(plan, fmt, chans_w=None):
+    chans = []
+    for i, c in enumerate(plan.channels):
+        w = plan.get_weights(i).astype(np.complex128) if chans_w is None else chans_w[i]
+        chans.append(oracle64.Channel(c["bins"], c["first"], w))
+    return oracle64.Oracle64(fmt, plan.fft_size, plan.ffts_per_buf, plan.averages, chans)
+
+
+def make_plan(fs, N, fmt, filters, B, averages, spec="f32", mode="batched", fc=0.0):
+    return Plan(fs, N, fmt, filters, fc_in=fc, ffts_per_buf=B, averages=averages, spectrum_format=spec, mode=mode)
+
+
+def run_compare(plan, fmt, raws, o64=None, tol=TOL, check_o32=None):
+    o64 = o64 or _o64(plan, fmt)
+    worst = 0.0
+    for raw in raws:
+        sp, outs = plan.process(raw)
+        sp64, outs64 = o64.process(raw)
+        assert [s for s, _ in sp] == [s for s, _ in sp64]
+        for (_, a), (_, r) in zip(sp, sp64):
+            if plan.spectrum_format == 2:
+                e = rel_rms(a, r)
+                worst = max(worst, e)
+                assert e < tol, e
+            else:
+                q = oracle64.quantize(10 * np.log10(r), "u8" if plan.spectrum_format == 0 else "u16")
+                assert np.max(np.abs(a.astype(np.int64) - q.astype(np.int64))) <= 1
+        for c, (a, r) in enumerate(zip(outs, outs64)):
+            assert a.shape == r.shape
+            e = rel_rms(a, r)
+            worst = max(worst, e)
+            assert e < tol, (c, plan.channels[c], e)
+        if check_o32 is not None:
+            sp32, outs32 = check_o32.process(raw)
+            for a, r in zip(outs, outs32):
+                assert rel_rms(a, r) < 2 * tol
+    return worst
+
+
+def test_c1_plain_small_vs_oracles():
+    w = workloads.c1()
+    nbuf = 12
+    raw = workloads.stream_numpy(w, 0, nbuf * w.samples_per_buffer)
+    raws = np.split(raw.view(np.uint8), nbuf)
+    for mode in ("plain", "batched"):
+        plan = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages, mode=mode)
+        assert [c["bins"] for c in plan.channels] == [256] * 4
+        o32 = oracle32.Oracle32(w.fs, w.fc, w.fft_size, w.ffts_per_buf, w.averages, w.fmt, w.filters())
+        assert [(c["bins"], c["first"]) for c in plan.channels] == o32.channels
+        worst = run_compare(plan, w.fmt, raws, check_o32=o32)
+        print(f"c1 {mode}: worst rel rms {worst:.2e}")
+
+
+@pytest.mark.parametrize("fmt", sorted(oracle64.FORMATS))
+def test_all_formats_small(fmt):
+    rng = np.random.default_rng(oracle64.fmt_code(fmt))
+    N, B, avg = 1024, 6, 4
+    cplx = oracle64.is_complex(fmt)
+    chans = [(64, 100), (128, -300 if cplx else 260), (32, 480), (256, 8), (4, 14), (1024, 512), (16, -8)]
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * (first + n // 2)) for n, first in chans]
+    plan = make_plan(1024e3, N, fmt, filters, B, avg)
+    assert plan.n_channels == len(chans)
+    from tests.test_oracle import _stream
+    raws = [_stream(fmt, plan.new_samples, rng) for _ in range(5)]
+    run_compare(plan, fmt, raws)
+
+
+@pytest.mark.parametrize("fmt,N", [("s16le", 32768), ("s16le", 65536), ("cs16le", 4096),
+                                   ("cs16le", 16384), ("cs16le", 65536), ("s16le", 8192), ("s16le", 16)])
+def test_fft_sizes_and_split_paths(fmt, N):
+    """Single-tile FFTs, the residue-split path (Nc = R1 * 8192, R1 = 2..8),
+    and the smallest size."""
+    rng = np.random.default_rng(N)
+    B = 4
+    fs = float(N) * 1000.0
+    cplx = fmt.startswith("c")
+    ns = [n for n in (4, 64, 512, 2048, 8192) if n <= max(4, N // 2)]
+    filters = []
+    for n in ns:
+        centre = 4 * int(rng.integers(-N // 8, N // 8)) if cplx else 4 * int(rng.integers(0, N // 8 + 1))
+        filters.append(dict(fs_out=1000.0 * n, fc_out=1000.0 * centre))
+    plan = make_plan(fs, N, fmt, filters, B, 3)
+    from tests.test_oracle import _stream
+    raws = [_stream(fmt, plan.new_samples, rng) for _ in range(3)]
+    run_compare(plan, fmt, raws)
+
+
+@pytest.mark.parametrize("spec", ["u8", "u16"])
+def test_quantised_spectra(spec):
+    w = workloads.c1()
+    raw = workloads.stream_numpy(w, 0, 8 * w.samples_per_buffer).view(np.uint8)
+    plan = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 16, spec=spec)
+    run_compare(plan, w.fmt, np.split(raw, 8))
+
+
+def test_edge_channels_wrap_mirror_and_drops():
+    """Channels across bin 0 and across Nyquist (conjugate mirror), wider than
+    half the spectrum, smallest and largest sizes; inexact and unsupported
+    filters are dropped with their status (fcfb.rs:58-61)."""
+    N, B = 4096, 4
+    fs = 4.096e6
+    filters = [
+        dict(fs_out=256e3, fc_out=0.0),                 # centred on bin 0: wraps to negative bins
+        dict(fs_out=512e3, fc_out=2048e3),              # centred on Nyquist: mirrored bins
+        dict(fs_out=8192e3, fc_out=1000e3),             # n = 8192 > N: wraps more than once
+        dict(fs_out=4e3, fc_out=100e3),                 # n = 4
+        dict(fs_out=64e3, fc_out=1001e3),               # centre not a multiple of 4: dropped
+        dict(fs_out=48e3, fc_out=0.0),                  # n = 48: exact, but not a power of two
+        dict(fs_out=-4e3, fc_out=0.0),                  # bins <= 0: dropped
+    ]
+    plan = make_plan(fs, N, "s16le", filters, B, 5)
+    assert plan.filter_status[:4] == [0, 0, 0, 0]
+    assert plan.filter_status[4] == SK_ERR_FILTER and plan.filter_status[6] == SK_ERR_FILTER
+    assert plan.filter_status[5] == SK_ERR_UNSUPPORTED
+    o32 = oracle32.Oracle32(fs, 0.0, N, B, 5, "s16le", filters)
+    assert o32.filter_status[4] != 0 and o32.filter_status[6] != 0 and o32.filter_status[5] == 0
+    assert [(c["bins"], c["first"]) for c in plan.channels] == [o32.channels[i] for i in (0, 1, 2, 3)]
+    rng = np.random.default_rng(11)
+    from tests.test_oracle import _stream
+    run_compare(plan, "s16le", [_stream("s16le", plan.new_samples, rng) for _ in range(4)])
+
+
+def test_invalid_parameters_rejected():
+    with pytest.raises(SpektriError):
+        Plan(1e6, 1024, "s16le", [], ffts_per_buf=3)          # odd fftbuf with real input
+    with pytest.raises(SpektriError):
+        Plan(1e6, 1000, "s16le", [], ffts_per_buf=2)          # not a power of two
+    with pytest.raises(SpektriError):
+        Plan(1e6, 1 << 20, "s16le", [], ffts_per_buf=2)       # beyond the residue-split limit
+    p = Plan(1e6, 1024, "cs16le", [], ffts_per_buf=3)        # odd is fine for complex input
+    assert p.n_channels == 0
+    p.process(np.zeros(p.raw_bytes, np.uint8))
+
+
+def test_c3_shape_plain_equals_batched_and_oracle():
+    """The batching configuration (N=65536, 256 channels of 64..8192, B=64):
+    two buffers against the FP64 oracle; plain and batched bit-identical."""
+    w = workloads.c3()
+    x = workloads.stream_torch(w, 2 * w.samples_per_buffer, "cuda").cpu().numpy()
+    raws = np.split(x, 2)
+    pb = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages, mode="batched")
+    pp = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages, mode="plain")
+    assert pb.n_channels == 256
+    o64 = _o64(pb, w.fmt)
+    for r in raws:
+        sb, ob = pb.process(r)
+        sp, op = pp.process(r)
+        s64, o = o64.process(r)
+        for a, b in zip(ob, op):
+            assert np.array_equal(a, b)
+        errs = [rel_rms(a, ref) for a, ref in zip(ob, o)]
+        assert max(errs) < TOL, max(errs)
+
+
+def test_device_path_matches_host_path():
+    w = workloads.c1()
+    raw = workloads.stream_numpy(w, 0, 3 * w.samples_per_buffer).view(np.uint8)
+    ph = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 8)
+    pd = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 8)
+    for r in np.split(raw, 3):
+        sh, oh = ph.process(r)
+        rd = torch.from_numpy(r.copy()).cuda()
+        outs = [torch.empty(c["out_samples"], dtype=torch.complex64, device="cuda") for c in pd.channels]
+        spec = torch.empty(pd.max_spectra * pd.spectrum_bytes, dtype=torch.uint8, device="cuda")
+        res = pd.process_device(rd, outs, spec)
+        torch.cuda.synchronize()
+        assert res.n_spectra == len(sh)
+        for a, b in zip(oh, outs):
+            assert np.array_equal(a, b.cpu().numpy())
+        if sh:
+            s = pd.split_spectra(spec.cpu().numpy(), res)
+            for (q1, a), (q2, b) in zip(sh, s):
+                assert q1 == q2 and np.array_equal(a, b)
+
+
+def test_weights_update_and_custom_complex_weights():
+    w = workloads.c1()
+    raw = workloads.stream_numpy(w, 0, 2 * w.samples_per_buffer).view(np.uint8)
+    rng = np.random.default_rng(9)
+    cw = [(rng.standard_normal(256) + 1j * rng.standard_normal(256)).astype(np.complex64) for _ in w.channels]
+    filt = [dict(f, weights=cw[i]) for i, f in enumerate(w.filters())]
+    plan = make_plan(w.fs, w.fft_size, w.fmt, filt, w.ffts_per_buf, 64)
+    for i in range(plan.n_channels):
+        assert np.array_equal(plan.get_weights(i), cw[i])
+    o64 = _o64(plan, w.fmt, [c.astype(np.complex128) for c in cw])
+    r0, r1 = np.split(raw, 2)
+    run_compare(plan, w.fmt, [r0], o64=o64)
+    new = (rng.standard_normal(256) + 1j * rng.standard_normal(256)).astype(np.complex64)
+    plan.set_weights(2, new)
+    o64.channels[2].weights = new.astype(np.complex128)
+    run_compare(plan, w.fmt, [r1], o64=o64)
