@@ -101,7 +101,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "from the untimed pre-roll through the end of the timed region"}
 
 
 def dist_setup():
@@ -199,6 +200,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--compare-plain", action="store_true", help="also time the plain per-channel path")
+    ap.add_argument("--ffts-per-buf", type=int, default=0, help="override blocks per buffer (small profiling cases)")
+    ap.add_argument("--preroll", type=float, default=1.5, help="seconds of untimed steps while clocks are sampled")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_setup()
@@ -212,6 +215,8 @@ def main():
     dev = local
     torch.cuda.set_device(dev)
     w = workloads.WORKLOADS[args.workload]()
+    if args.ffts_per_buf:
+        w.ffts_per_buf = args.ffts_per_buf
     w.seed += 7919 * rank                                 # each replica its own stream
     spb = w.samples_per_buffer
     nbuf = min(DISTINCT_BUFFERS, w.n_samples // spb)
@@ -235,10 +240,19 @@ def main():
 
     run_steps(plan, args.warmup, 0)
     torch.cuda.synchronize(dev)
-    barrier(ws)
-    torch.cuda.synchronize(dev)
+    # Clock samples: the sampler starts during an untimed pre-roll of the same
+    # steps (>= 1 s, so nvidia-smi has samples under load) and runs to the end
+    # of the timed region.
     clocks = ClockSampler(dev)
     clocks.start()
+    t_pre = time.perf_counter()
+    k_pre = 0
+    while time.perf_counter() - t_pre < args.preroll:
+        run_steps(plan, 20, k_pre)
+        torch.cuda.synchronize(dev)
+        k_pre += 20
+    barrier(ws)
+    torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     run_steps(plan, args.steps, args.warmup)

@@ -308,7 +308,8 @@ __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
     }
     __syncthreads();
     tile_fft<+1, S, T>(sm, a.tw, log2n);
-    const int lo = n >> 3, keep = n - 2 * lo;                   // fcfb.rs:177
+    // fcfb.rs:177 keeps [n/8, 7(n/8)): 6(n/8) samples (none for n = 4)
+    const int lo = n >> 3, keep = 6 * lo;
 #pragma unroll 4
     for (int k = 0; k < E; ++k) {
       const int e = threadIdx.x + k * T;
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(T, 2) fcfb_backward_kernel(BwdArgs a) {
   const int N = 1 << a.log2N;
   const TileDesc td = a.tiles[blockIdx.x];
   const int log2n = td.log2n, n = 1 << log2n, half = n >> 1;
-  const int lo = n >> 3, keep = n - 2 * lo;
+  const int lo = n >> 3, keep = 6 * lo;
   for (int k = 0; k < E; ++k) {
     const int e = threadIdx.x + k * T;
     const int t = e >> log2n, i = e & (n - 1);

@@ -194,6 +194,39 @@ def test_device_path_matches_host_path():
                 assert q1 == q2 and np.array_equal(a, b)
 
 
+def test_outputs_stay_inside_their_buffers():
+    """Channel outputs are packed into one tensor with sentinel gaps between
+    them; after processing every gap still holds its sentinel (n = 4 keeps
+    no samples at all, fcfb.rs:177)."""
+    N, B = 1024, 4
+    sizes = [4, 8, 16, 64, 1024, 4, 8192]
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * (i + 3)) for i, n in enumerate(sizes)]
+    for mode in ("batched", "plain"):
+        plan = make_plan(1024e3, N, "s16le", filters, B, 3, mode=mode)
+        assert plan.n_channels == len(sizes)
+        assert [c["out_samples"] for c in plan.channels] == [B * (n // 8 * 6) for n in sizes]
+        gap = 256
+        total = sum(c["out_samples"] for c in plan.channels) + gap * (len(sizes) + 1)
+        big = torch.full((total,), complex(12345.0, -6789.0), dtype=torch.complex64, device="cuda")
+        outs, gaps, o = [], [], gap
+        gaps.append((0, gap))
+        for c in plan.channels:
+            outs.append(big[o:o + c["out_samples"]])
+            o += c["out_samples"]
+            gaps.append((o, o + gap))
+            o += gap
+        spec = torch.empty(plan.max_spectra * plan.spectrum_bytes + 4096, dtype=torch.uint8, device="cuda")
+        spec[plan.max_spectra * plan.spectrum_bytes:] = 77
+        rng = np.random.default_rng(1)
+        for _ in range(3):
+            raw = torch.from_numpy(np.clip(rng.normal(0, 3000, plan.new_samples), -32768, 32767).astype("<i2").view(np.uint8)).cuda()
+            plan.process_device(raw, outs, spec)
+        torch.cuda.synchronize()
+        for a, b in gaps:
+            assert torch.all(big[a:b] == complex(12345.0, -6789.0)), (mode, a, b)
+        assert torch.all(spec[plan.max_spectra * plan.spectrum_bytes:] == 77)
+
+
 def test_weights_update_and_custom_complex_weights():
     w = workloads.c1()
     raw = workloads.stream_numpy(w, 0, 2 * w.samples_per_buffer).view(np.uint8)
