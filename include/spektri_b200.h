@@ -201,6 +201,28 @@ int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W
 int sk_plan_set_timing(sk_plan* plan, int enable);
 int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
 
+/* ------------------------------------------------------------ allocation-free spectra
+ * No counterpart in the reference: an addition for callers that may not
+ * allocate device memory — a real-time receive callback that must never
+ * stall on cudaMalloc (it can synchronise the GPU for milliseconds and drop
+ * samples), or a host application whose own pool owns the whole device
+ * budget.  Same forward spectra as sk_spectra_device, with no plan and no
+ * allocation: the FFT intermediates and twiddles live in one static device
+ * array of SK_NOALLOC_SCRATCH_ELEMS complex floats (8 MiB) that every GPU
+ * loading the library keeps until exit.
+ *   raw : device, fft_size/4 + 3*fft_size/4 * n_blocks samples of
+ *         input_format (the N/4 samples carried from the previous window
+ *         come first, as in the reference's buffer, main.rs:162-181)
+ *   X   : device, n_blocks * K complex64 spectra, K = N/2+1 (real) or N
+ * Limit: 8192 + N + n_blocks * Nc <= SK_NOALLOC_SCRATCH_ELEMS (Nc = N/2 for
+ * real input, N for complex); larger requests return SK_ERR_ARG.  All calls
+ * share the array: calls whose work overlaps on the GPU race.  The first call
+ * on each device looks up the array's address and makes synchronous runtime
+ * calls, so make it before any stream capture. */
+#define SK_NOALLOC_SCRATCH_ELEMS 1048576
+int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_t fft_size, uint32_t n_blocks,
+                       float* X, void* stream);
+
 /* Pinned host memory for staging (cudaHostAlloc); NULL on failure. */
 void* sk_host_alloc(size_t bytes);
 void sk_host_free(void* p);

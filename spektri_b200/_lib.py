@@ -92,6 +92,7 @@ PROTOTYPES = [
                                           C.c_void_p, C.c_void_p]),
     ("sk_plan_set_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("sk_plan_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    ("sk_spectra_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("sk_host_alloc", C.c_void_p, [C.c_size_t]),
     ("sk_host_free", None, [C.c_void_p]),
 ]

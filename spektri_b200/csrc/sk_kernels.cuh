@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(256) welch_split_kernel(SplitArgs a) {
 // written (spectrum.rs:116-161) and the accumulator restarts.  fmt: 0 u8,
 // 1 u16 big-endian, 2 f32 mean power.  The u8/u16 arithmetic is rounded per
 // operation (no fused multiply-add) like the reference.
-__global__ void __launch_bounds__(256) welch_accum_kernel(const float* __restrict__ P, float* acc, int K, int B,
+static __global__ void __launch_bounds__(256) welch_accum_kernel(const float* __restrict__ P, float* acc, int K, int B,
                                                           int accn0, int averages, int fmt, float db_plus,
                                                           uint8_t* out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;

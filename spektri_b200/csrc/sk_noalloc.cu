@@ -1,0 +1,210 @@
+// Allocation-free forward spectra: sk_spectra_noalloc.
+//
+// Who needs this.  Some programs that embed the filter bank may not call
+// cudaMalloc at all: an SDR receive callback that must never stall (a device
+// allocation can synchronise the whole GPU and take milliseconds, long enough
+// to drop samples), or a host application that hands its entire device
+// memory budget to its own pool at start-up and forbids libraries from
+// allocating behind its back.  The plan-based API allocates its scratch when
+// a plan is created, so those callers cannot use it.  This entry point gives
+// them the forward FFT stage with no allocation: the caller passes the raw
+// input and the output spectra, and the intermediate FFT results and twiddle
+// tables live in one fixed array compiled into the library.
+//
+// The array is g_noalloc_scratch below: SK_NOALLOC_SCRATCH_ELEMS complex
+// floats (8 MiB), reserved on every GPU that loads the library until the
+// process exits.  All calls on a device share it and it keeps whatever the
+// last call left there; every call rewrites the parts it reads (twiddles
+// first, then the FFT results), so nothing has to start at zero.  Two calls
+// whose work overlaps on the GPU (different streams, or different host
+// threads on the same device) race on the array and corrupt each other.
+//
+// Host code cannot use the array's name as a device address (in host code it
+// names a host-side shadow), so the first call on each device looks up the
+// real address with cudaGetSymbolAddress, with that device current, and sets
+// the kernels' shared-memory limits.  That first call therefore makes
+// synchronous runtime calls; make it before any stream capture begins.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "spektri_b200.h"
+#include "sk_internal.h"
+#include "sk_kernels.cuh"
+
+using namespace sk;
+
+namespace {
+
+constexpr int S = TILE_S;
+constexpr int T = TILE_T;
+constexpr size_t TILE_SMEM = TileShape<S>::SMEM_BYTES;
+constexpr size_t kScratchElems = SK_NOALLOC_SCRATCH_ELEMS;
+
+static __device__ __align__(256) float2 g_noalloc_scratch[kScratchElems];
+
+struct DeviceSetup {
+  bool ready = false;
+  float2* base = nullptr;     // device address of g_noalloc_scratch on this device
+};
+std::mutex g_mu;
+std::vector<DeviceSetup> g_setup;
+
+// W_n^k = exp(-2 pi i k / n) for the tile table (n = S) and the window table.
+__global__ void noalloc_twiddles(float2* tw_tile, float2* tw_big, int n_big) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s, c;
+  if (i < S) {
+    sincospi(-2.0 * (double)i / (double)S, &s, &c);
+    tw_tile[i] = make_float2((float)c, (float)s);
+  }
+  if (i < n_big) {
+    sincospi(-2.0 * (double)i / (double)n_big, &s, &c);
+    tw_big[i] = make_float2((float)c, (float)s);
+  }
+}
+
+using FwdFn = void (*)(FwdArgs);
+template <int FMT>
+FwdFn fwd_for() { return fwd_fft_kernel<S, T, FMT>; }
+FwdFn fwd_kernel(int fmt) {
+  switch (fmt) {
+    case SK_FMT_S8: return fwd_for<SK_FMT_S8>();
+    case SK_FMT_S16LE: return fwd_for<SK_FMT_S16LE>();
+    case SK_FMT_S16BE: return fwd_for<SK_FMT_S16BE>();
+    case SK_FMT_F32LE: return fwd_for<SK_FMT_F32LE>();
+    case SK_FMT_F32BE: return fwd_for<SK_FMT_F32BE>();
+    case SK_FMT_U8: return fwd_for<SK_FMT_U8>();
+    case SK_FMT_CS8: return fwd_for<SK_FMT_CS8>();
+    case SK_FMT_CS16LE: return fwd_for<SK_FMT_CS16LE>();
+    case SK_FMT_CS16BE: return fwd_for<SK_FMT_CS16BE>();
+    case SK_FMT_CF32LE: return fwd_for<SK_FMT_CF32LE>();
+    case SK_FMT_CF32BE: return fwd_for<SK_FMT_CF32BE>();
+    case SK_FMT_CU8: return fwd_for<SK_FMT_CU8>();
+  }
+  return nullptr;
+}
+
+int log2_exact(long long v) {
+  if (v <= 0 || (v & (v - 1))) return -1;
+  int r = 0;
+  while ((1ll << r) < v) ++r;
+  return r;
+}
+
+// Once per device, with that device current: the array's device address and
+// the kernels' dynamic shared-memory limit.
+int setup_device(int dev, float2** base) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((int)g_setup.size() <= dev) g_setup.resize(dev + 1);
+  DeviceSetup& d = g_setup[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+    static const int fmts[] = {SK_FMT_S8, SK_FMT_S16LE, SK_FMT_S16BE, SK_FMT_F32LE, SK_FMT_F32BE, SK_FMT_U8,
+                               SK_FMT_CS8, SK_FMT_CS16LE, SK_FMT_CS16BE, SK_FMT_CF32LE, SK_FMT_CF32BE, SK_FMT_CU8};
+    for (int f : fmts) {
+      e = cudaFuncSetAttribute(fwd_kernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
+      if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
+    d.base = (float2*)p;
+    d.ready = true;
+  }
+  *base = d.base;
+  return SK_OK;
+}
+
+}  // namespace
+
+extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_t fft_size, uint32_t n_blocks,
+                                  float* X, void* stream) {
+  if (!raw || !X) return fail(SK_ERR_ARG, "sk_spectra_noalloc: null raw input or output");
+  if (!format_valid(input_format)) return fail(SK_ERR_ARG, "sk_spectra_noalloc: unknown input format 0x%02x", input_format);
+  if (n_blocks == 0) return fail(SK_ERR_ARG, "sk_spectra_noalloc: n_blocks must be positive");
+  const bool cplx = format_complex(input_format);
+  const int log2N = log2_exact(fft_size);
+  const int log2Nc = log2N - (cplx ? 0 : 1);
+  if (log2N < 3 || log2Nc < 2 || log2Nc > TileShape<S>::LOGS + 3)
+    return fail(SK_ERR_UNSUPPORTED, "sk_spectra_noalloc: FFT size %u not supported (power of two, 8 .. %d complex points)",
+                fft_size, 1 << (TileShape<S>::LOGS + 3));
+  if ((uintptr_t)raw % (format_bits(input_format) / 8))
+    return fail(SK_ERR_ARG, "sk_spectra_noalloc: raw input misaligned for its sample format");
+  const long long N = fft_size, Nc = 1ll << log2Nc;
+  const unsigned long long need = (unsigned long long)S + (unsigned long long)N + (unsigned long long)n_blocks * Nc;
+  if (need > kScratchElems)
+    return fail(SK_ERR_ARG,
+                "sk_spectra_noalloc: %u blocks of FFT size %u need %llu complex scratch elements; the static "
+                "scratch holds %zu (%zu MiB): at most %lld blocks at this size",
+                n_blocks, fft_size, need, kScratchElems, kScratchElems * sizeof(float2) >> 20,
+                (long long)((kScratchElems - S - N) / Nc));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  float2* base = nullptr;
+  int rc = setup_device(dev, &base);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  float2* tw_tile = base;
+  float2* tw_big = base + S;
+  float2* Z = base + S + N;
+
+  const int nt = (int)std::max<long long>(S, N);
+  noalloc_twiddles<<<(nt + 255) / 256, 256, 0, st>>>(tw_tile, tw_big, (int)N);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SK_ERR_CUDA, "twiddle kernel: %s", cudaGetErrorString(e));
+
+  // The caller's window holds every sample: [N/4 carried | 3N/4 * n_blocks new].
+  const long long hop = N - N / 4;
+  FwdArgs a{};
+  a.raw = (const uint8_t*)raw;
+  a.halo = nullptr;
+  a.halo_next = nullptr;
+  a.overlap = 0;                       // no carry: the window starts at sample 0 of block 0
+  a.nnew = hop * n_blocks + N / 4;
+  a.hop = (int)hop;
+  a.B = (int)n_blocks;
+  a.log2N = log2N;
+  a.log2Nc = log2Nc;
+  a.R1 = 1;
+  a.log2R1 = 0;
+  if (log2Nc > TileShape<S>::LOGS) {
+    a.log2R1 = log2Nc - TileShape<S>::LOGS;
+    a.R1 = 1 << a.log2R1;
+  }
+  a.wscale = format_scaling(input_format) / (float)N;
+  a.tw_tile = tw_tile;
+  a.tw_big = tw_big;
+  a.Z = Z;
+  int grid;
+  if (a.R1 == 1) {
+    const int per = S >> log2Nc;
+    grid = (int)((n_blocks + per - 1) / per);
+  } else {
+    grid = (int)n_blocks * a.R1;
+  }
+  fwd_kernel(input_format)<<<grid, T, TILE_SMEM, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SK_ERR_CUDA, "forward FFT kernel: %s", cudaGetErrorString(e));
+
+  SplitArgs s{};
+  s.Z = Z;
+  s.X = (float2*)X;
+  s.P = nullptr;
+  s.log2N = log2N;
+  s.log2Nc = log2Nc;
+  s.K = cplx ? (int)N : (int)(N / 2 + 1);
+  s.R1 = a.R1;
+  s.log2R1 = a.log2R1;
+  s.logS = TileShape<S>::LOGS;
+  s.tw_big = tw_big;
+  dim3 g2((s.K + 255) / 256, n_blocks);
+  if (cplx) welch_split_kernel<false><<<g2, 256, 0, st>>>(s);
+  else welch_split_kernel<true><<<g2, 256, 0, st>>>(s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SK_ERR_CUDA, "spectrum split kernel: %s", cudaGetErrorString(e));
+  return SK_OK;
+}
