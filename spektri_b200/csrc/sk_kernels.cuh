@@ -14,6 +14,7 @@
 //   fcfb_backward_kernel adjoint of fcfb_kernel for weight design
 #pragma once
 #include "sk_fft.cuh"
+#include "sk_fcfb.cuh"
 
 namespace sk {
 
@@ -274,14 +275,15 @@ struct FcfbArgs {
 template <int S, int T, bool PERSIST, bool REAL>
 __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
   extern __shared__ float2 sm[];
+  __shared__ TileMeta s_meta[MAX_TILE_TRANSFORMS];
   __shared__ int s_tile;
-  constexpr int E = S / T;
-  const int N = 1 << a.log2N;
+  static_assert(MAX_TILE_TRANSFORMS <= T, "one thread stages one transform's metadata");
   for (int it = 0;; ++it) {
+    const FcfbTileConst c{1 << a.log2N, a.K, a.tw};
     int tile;
     if constexpr (PERSIST) {
       if (threadIdx.x == 0) s_tile = atomicAdd(a.cursor, 1);
-      __syncthreads();
+      __syncthreads();               // also orders the previous tile's reads before this tile's writes
       tile = s_tile;
       if (tile >= a.ntiles) return;
     } else {
@@ -289,36 +291,20 @@ __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
       tile = tile_base + blockIdx.x;
     }
     const TileDesc td = a.tiles[tile];
-    const int log2n = td.log2n, n = 1 << log2n, half = n >> 1;
-#pragma unroll 4
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      const int t = e >> log2n, i = e & (n - 1);
-      float2 v = make_float2(0.f, 0.f);
-      if (t < td.count) {
-        const int2 cb = __ldg(&a.list[td.list_off + t]);
-        const ChanDev* ch = a.chans + cb.x;
-        const int j = (i + half) & (n - 1);                     // fcfb.rs:166-169
-        const int m = (int)((ch->first + j) & (long long)(N - 1));
-        const float2* Xb = a.X + (size_t)cb.y * a.K;
-        const float2 x = (REAL && m >= a.K) ? cconj(__ldg(&Xb[N - m])) : __ldg(&Xb[m]);
-        v = cmul(__ldg(&ch->w[j]), x);
-      }
-      sm[padx(e)] = v;
+    if (threadIdx.x < td.count) {
+      const int2 cb = __ldg(&a.list[td.list_off + threadIdx.x]);
+      const ChanDev& ch = a.chans[cb.x];
+      const int keep = 6 * ((1 << td.log2n) >> 3);
+      TileMeta m;
+      m.X = a.X + (size_t)cb.y * a.K;
+      m.w = ch.w;
+      m.out = ch.out + (size_t)cb.y * keep;
+      m.first = (int)(ch.first & (long long)(c.N - 1));
+      m.pad = 0;
+      s_meta[threadIdx.x] = m;
     }
     __syncthreads();
-    tile_fft<+1, S, T>(sm, a.tw, log2n);
-    // fcfb.rs:177 keeps [n/8, 7(n/8)): 6(n/8) samples (none for n = 4)
-    const int lo = n >> 3, keep = 6 * lo;
-#pragma unroll 4
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      const int t = e >> log2n, i = e & (n - 1);
-      if (t < td.count && i >= lo && i < lo + keep) {
-        const int2 cb = __ldg(&a.list[td.list_off + t]);
-        a.chans[cb.x].out[(size_t)cb.y * keep + (i - lo)] = sm[padx(e)];
-      }
-    }
+    fcfb_tile_dispatch<S, T, REAL>(td.log2n, sm, s_meta, td.count, c);
   }
 }
 

@@ -434,7 +434,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   std::vector<int2> list;
   std::vector<TileDesc> tiles;
   for (int l2 = TileShape<S>::LOGS; l2 >= 2; --l2) {
-    const int per = S >> l2;
+    const int per = std::min(S >> l2, MAX_TILE_TRANSFORMS);
     const int base = (int)list.size();
     for (size_t c = 0; c < pl->ch.size(); ++c)
       if (pl->ch[c].log2n == l2)
@@ -444,7 +444,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   }
   pl->n_batched_tiles = (int)tiles.size();
   for (size_t c = 0; c < pl->ch.size(); ++c) {
-    const int l2 = pl->ch[c].log2n, per = S >> l2;
+    const int l2 = pl->ch[c].log2n, per = std::min(S >> l2, MAX_TILE_TRANSFORMS);
     const int base = (int)list.size();
     for (int b = 0; b < pl->B; ++b) list.push_back(make_int2((int)c, b));
     pl->plain_start.push_back((int)tiles.size());
@@ -538,7 +538,8 @@ int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void*
   // Channel output pointers (re-uploaded only when they change).
   bool changed = false;
   for (size_t c = 0; c < pl->ch.size(); ++c) {
-    if (!chan_out[c]) return fail(SK_ERR_ARG, "null output for channel %zu", c);
+    // A channel of n = 4 keeps no samples (fcfb.rs:177): its output may be null.
+    if (!chan_out[c] && pl->ch[c].n >= 8) return fail(SK_ERR_ARG, "null output for channel %zu", c);
     if ((uintptr_t)chan_out[c] % 8) return fail(SK_ERR_ARG, "channel %zu output must be 8-byte aligned", c);
     pl->h_chans[c].out = (float2*)chan_out[c];
     if (pl->h_chans[c].out != pl->h_chans_uploaded[c].out) changed = true;
@@ -577,7 +578,7 @@ int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_o
   if (!raw) return fail(SK_ERR_ARG, "null raw input");
   if (!pl->ch.empty() && !chan_out) return fail(SK_ERR_ARG, "null channel output table");
   for (size_t c = 0; c < pl->ch.size(); ++c)
-    if (!chan_out[c]) return fail(SK_ERR_ARG, "null output for channel %zu", c);
+    if (!chan_out[c] && pl->ch[c].n >= 8) return fail(SK_ERR_ARG, "null output for channel %zu", c);
   DeviceGuard g(pl->p.device);
   cudaStream_t st = pl->stream;
   SK_CUDA(cudaMemcpyAsync(pl->d_raw, raw, pl->raw_bytes, cudaMemcpyHostToDevice, st));
@@ -588,6 +589,7 @@ int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_o
   if (rc) return rc;
   for (size_t c = 0; c < pl->ch.size(); ++c) {
     const size_t bytes = sizeof(float2) * (size_t)pl->B * (pl->ch[c].n / 8 * 6);
+    if (bytes == 0) continue;
     SK_CUDA(cudaMemcpyAsync(chan_out[c], pl->d_out + pl->ch[c].out_off, bytes, cudaMemcpyDeviceToHost, st));
   }
   if (r.n_spectra)
