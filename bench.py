@@ -270,7 +270,7 @@ def main():
     run_steps(plan, kt, 0)
     stage_ms, calls = plan.timing()
     plan.set_timing(False)
-    fcfb_ms = stage_ms[3] / max(1, calls)
+    fcfb_ms = stage_ms[2] / max(1, calls)
     out_bytes = sum(c["out_samples"] for c in plan.channels) * 8
     hbm, peak_kind = peaks()
     achieved = out_bytes / (fcfb_ms / 1e3) / 1e9
@@ -288,7 +288,7 @@ def main():
                          f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2"},
         "hbm_gbs_pipeline": round(value * 1e6 / ws * alg / 1e9, 1),
         "alg_bytes_per_sample": round(alg, 3),
-        "stage_ms": {k: round(v / max(1, calls), 4) for k, v in zip(["fwd_fft", "welch_split", "welch_accum", "fcfb"], stage_ms)},
+        "stage_ms": {k: round(v / max(1, calls), 4) for k, v in zip(["fwd_fft", "welch", "fcfb"], stage_ms)},
         "roofline": {"bound": "hbm", "kernel": "fcfb_kernel (persistent)", "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "peak_kind": f"{peak_kind} copy bandwidth", "traffic": None,

@@ -193,11 +193,11 @@ int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W
                             float* const* dW, float* dX, void* stream);
 
 /* Per-stage device timing with CUDA events recorded on the launching stream
- * (off by default).  Stages: 0 forward FFT, 1 spectrum split + Welch terms,
- * 2 Welch accumulation, 3 filter bank.  sk_plan_timing waits for the
- * recorded work, returns the summed milliseconds per stage and the number of
- * calls measured, and resets the totals. */
-#define SK_N_STAGES 4
+ * (off by default).  Stages: 0 forward FFT, 1 spectrum split + Welch
+ * accumulation, 2 filter bank.  sk_plan_timing waits for the recorded work,
+ * returns the summed milliseconds per stage and the number of calls
+ * measured, and resets the totals. */
+#define SK_N_STAGES 3
 int sk_plan_set_timing(sk_plan* plan, int enable);
 int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
 

@@ -5,7 +5,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def build(jobs: int = 2) -> None:
+def build(jobs: int = 8) -> None:
     subprocess.run(["make", "-s", "-j", str(jobs), "-C", HERE], check=True)
 
 

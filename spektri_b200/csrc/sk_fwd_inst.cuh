@@ -1,0 +1,22 @@
+// One forward-FFT kernel instance per input format; included by the
+// sk_fwd_{8,16,32}.cu units, which split the formats by sample width so the
+// instances compile in parallel.
+#pragma once
+#include "spektri_b200.h"
+#include "sk_kernels.cuh"
+
+namespace sk {
+
+template <int FMT>
+cudaError_t fwd_launch_one(int grid, const FwdArgs& a, cudaStream_t st) {
+  fwd_fft_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int FMT>
+cudaError_t fwd_prepare_one() {
+  return cudaFuncSetAttribute(fwd_fft_kernel<TILE_S, TILE_T, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TILE_SMEM);
+}
+
+}  // namespace sk

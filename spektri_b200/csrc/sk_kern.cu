@@ -1,0 +1,78 @@
+// Kernel instances and launchers for the spectrum split, the fused Welch
+// accumulation, the filter bank (plain and persistent) and its adjoint, plus
+// the per-width dispatch of the forward FFT.
+#include "sk_internal.h"
+#include "sk_kernels.cuh"
+
+namespace sk {
+
+cudaError_t fwd_prepare(int fmt) {
+  switch (format_bits(fmt)) {
+    case 8: return fwd_prepare_8(fmt);
+    case 16: return fwd_prepare_16(fmt);
+    case 32: return fwd_prepare_32(fmt);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
+  switch (format_bits(fmt)) {
+    case 8: return launch_fwd_8(fmt, grid, a, st);
+    case 16: return launch_fwd_16(fmt, grid, a, st);
+    case 32: return launch_fwd_32(fmt, grid, a, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) {
+  const dim3 g((s.K + 255) / 256, B);
+  if (cplx) welch_split_kernel<false><<<g, 256, 0, st>>>(s);
+  else welch_split_kernel<true><<<g, 256, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
+  constexpr int bins_per_cta = WELCH_WARP_BINS;
+  const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
+  if (cplx) welch_kernel<false><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
+  else welch_kernel<true><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
+  return cudaGetLastError();
+}
+
+cudaError_t fcfb_prepare() {
+  const void* fns[] = {(const void*)fcfb_kernel<TILE_S, TILE_T, true, true>,
+                       (const void*)fcfb_kernel<TILE_S, TILE_T, true, false>,
+                       (const void*)fcfb_kernel<TILE_S, TILE_T, false, true>,
+                       (const void*)fcfb_kernel<TILE_S, TILE_T, false, false>,
+                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
+                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>};
+  for (const void* f : fns) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t fcfb_occupancy(int* per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel<TILE_S, TILE_T, true, true>, TILE_T,
+                                                       TILE_SMEM);
+}
+
+cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st) {
+  if (persistent) {
+    if (cplx) fcfb_kernel<TILE_S, TILE_T, true, false><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
+    else fcfb_kernel<TILE_S, TILE_T, true, true><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
+  } else {
+    if (cplx) fcfb_kernel<TILE_S, TILE_T, false, false><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
+    else fcfb_kernel<TILE_S, TILE_T, false, true><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st) {
+  if (cplx) fcfb_backward_kernel<TILE_S, TILE_T, false><<<grid, TILE_T, TILE_SMEM, st>>>(a);
+  else fcfb_backward_kernel<TILE_S, TILE_T, true><<<grid, TILE_T, TILE_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace sk

@@ -13,35 +13,11 @@
 //                       times weights, inverse FFT, keep [n/8, 7n/8)        [fcfb.rs:154-188]
 //   fcfb_backward_kernel adjoint of fcfb_kernel for weight design
 #pragma once
+#include "sk_types.h"
 #include "sk_fft.cuh"
 #include "sk_fcfb.cuh"
 
 namespace sk {
-
-constexpr int TILE_S = 8192;   // complex elements per tile (64 KB + padding in shared memory)
-constexpr int TILE_T = 256;    // threads per tile CTA (32 elements per thread)
-
-struct ChanDev {               // one filter-bank channel, as the kernels see it
-  const float2* w;             // weights, natural order: w[j] scales bin first+j
-  float2* out;                 // B * 3n/4 outputs
-  long long first;
-  int log2n;
-  int pad;
-};
-struct BwdChan {
-  const float2* w;
-  const float2* dy;            // B * 3n/4 output gradients
-  float2* dw;                  // n weight gradients (accumulated)
-  long long first;
-  int log2n;
-  int pad;
-};
-struct TileDesc {              // S/n transforms of one size
-  int log2n;
-  int list_off;                // first entry in the (channel, block) list
-  int count;                   // transforms in this tile (<= S/n)
-  int pad;
-};
 
 // ----------------------------------------------------------------- input formats
 // One scalar component of a raw sample (inputformats.rs:65-155).  BASE is the
@@ -72,41 +48,73 @@ struct SampleSrc {
   const uint8_t* raw;
   const float* halo;
   long long overlap;
+  // Component loads stay scalar: measured on B200, one 32-bit load per s16le
+  // pair made the forward kernel 1.5x slower than two 16-bit loads.
   __device__ __forceinline__ float2 pair(long long p) const {
     constexpr int BASE = FMT & 0x3F;
     constexpr bool CPLX = (FMT & 0xC0) == 0x40;
     if (p < overlap) return *reinterpret_cast<const float2*>(halo + (CPLX ? 2 * p : p));
-    const long long q = p - overlap;
-    if constexpr (CPLX) return make_float2(load_comp<BASE>(raw, 2 * q), load_comp<BASE>(raw, 2 * q + 1));
-    return make_float2(load_comp<BASE>(raw, q), load_comp<BASE>(raw, q + 1));
+    const long long c = CPLX ? 2 * (p - overlap) : p - overlap;   // first component index
+    return make_float2(load_comp<BASE>(raw, c), load_comp<BASE>(raw, c + 1));
   }
 };
 
 // ----------------------------------------------------------------- forward FFT
-struct FwdArgs {
-  const uint8_t* raw;          // new samples of this buffer
-  const float* halo;           // converted last N/4 samples of the previous buffer
-  float* halo_next;            // receives the converted last N/4 samples of this one
-  long long overlap, nnew;
-  int hop, B;
-  int log2N, log2Nc;           // N (window length) and Nc (complex FFT length)
-  int R1, log2R1;              // Nc = R1 * S when Nc > S (R1 = 1 otherwise)
-  float wscale;                // rectangular window value scaling/N (dsp.rs:70-73)
-  const float2* tw_tile;       // W_S^k
-  const float2* tw_big;        // W_N^k, k < N
-  float2* Z;                   // [B][Nc]; for R1 > 1 element k1 + R1*k2 sits at k1*S + k2
-};
 
 // Tile = S/Nc whole blocks (Nc <= S), or one residue class k1 of one block
 // (Nc = R1*S): z'[j2] = W_Nc^{j2 k1} sum_j1 z[j1 S + j2] W_R1^{j1 k1}, whose
 // S-point DFT is Z[k1 + R1 k2] (the last radix-R1 stage done first, as
 // prototyping/parallel_fft.py:20-28 splits a 4-way FFT).
+// Whole blocks: S/Nc blocks per tile, Nc = 2^LOGN.
+template <int LOGN, int S, int T, int FMT>
+__device__ __forceinline__ void fwd_tile_blocks(float2* sm, const FwdArgs& a, const SampleSrc<FMT>& src, int tile) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int per = S >> LOGN;
+  const int b0 = tile * per;
+  const int count = min(per, a.B - b0);
+  auto load = [&](int t, int j) {
+    float2 z = src.pair((long long)(b0 + t) * a.hop + (CPLX ? j : 2 * j));   // x * scaling/N
+    return make_float2(z.x * a.wscale, z.y * a.wscale);
+  };
+  auto store = [&](int t, int o, float2 v) { a.Z[((size_t)(b0 + t) << LOGN) + o] = v; };
+  tile_pipeline<LOGN, S, T, -1>(sm, count, a.tw_tile, load, store);
+}
+
+// One residue class k1 of one block (Nc = R1 S): element j2 of the tile is
+// W_Nc^{j2 k1} sum_j1 z[j1 S + j2] W_R1^{j1 k1}.
+template <int LOGR1, int S, int T, int FMT>
+__device__ __forceinline__ void fwd_tile_split(float2* sm, const FwdArgs& a, const SampleSrc<FMT>& src, int tile) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int R1 = 1 << LOGR1, LOGS = ilog2c(S);
+  const int b = tile >> LOGR1, k1 = tile & (R1 - 1);
+  const int shR = a.log2N - LOGR1, shC = a.log2N - (LOGS + LOGR1);
+  const long long p0 = (long long)b * a.hop;
+  float2* Zb = a.Z + ((size_t)b << (LOGS + LOGR1)) + ((size_t)k1 << LOGS);
+  float2 rot[R1];                                    // W_R1^{j1 k1}: fixed for the tile
+#pragma unroll
+  for (int j1 = 0; j1 < R1; ++j1) rot[j1] = __ldg(&a.tw_big[((j1 * k1) & (R1 - 1)) << shR]);
+  auto load = [&](int, int e) {
+    float2 z[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; ++j1) {
+      const int jj = (j1 << LOGS) + e;
+      z[j1] = src.pair(p0 + (CPLX ? jj : 2 * jj));
+    }
+    float2 acc = make_float2(z[0].x * a.wscale, z[0].y * a.wscale);
+#pragma unroll
+    for (int j1 = 1; j1 < R1; ++j1)
+      acc = cadd(acc, cmul(make_float2(z[j1].x * a.wscale, z[j1].y * a.wscale), rot[j1]));
+    if (k1) acc = cmul(acc, __ldg(&a.tw_big[(e * k1) << shC]));
+    return acc;
+  };
+  auto store = [&](int, int o, float2 v) { Zb[o] = v; };
+  tile_pipeline<LOGS, S, T, -1>(sm, 1, a.tw_tile, load, store);
+}
+
 template <int S, int T, int FMT>
 __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
-  constexpr int E = S / T;
-  constexpr int LOGS = ilog2c(S);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry: convert the last N/4 new samples for the next buffer (main.rs:173)
     const long long stride = (long long)gridDim.x * T;
@@ -116,70 +124,31 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
       a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
   }
   const int tile = blockIdx.x;
-  const int Nc = 1 << a.log2Nc;
   if (a.R1 == 1) {
-    const int per = S >> a.log2Nc;
-    const int b0 = tile * per;
-#pragma unroll 4
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      const int b = b0 + (e >> a.log2Nc);
-      const int j = e & (Nc - 1);
-      float2 z = make_float2(0.f, 0.f);
-      if (b < a.B) {
-        z = src.pair((long long)b * a.hop + (CPLX ? j : 2 * j));
-        z.x *= a.wscale;
-        z.y *= a.wscale;
-      }
-      sm[padx(e)] = z;
-    }
-    __syncthreads();
-    tile_fft<-1, S, T>(sm, a.tw_tile, a.log2Nc);
-#pragma unroll 4
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      const int b = b0 + (e >> a.log2Nc);
-      if (b < a.B) a.Z[((size_t)b << a.log2Nc) + (e & (Nc - 1))] = sm[padx(e)];
+    switch (a.log2Nc) {
+      case 2: fwd_tile_blocks<2, S, T, FMT>(sm, a, src, tile); break;
+      case 3: fwd_tile_blocks<3, S, T, FMT>(sm, a, src, tile); break;
+      case 4: fwd_tile_blocks<4, S, T, FMT>(sm, a, src, tile); break;
+      case 5: fwd_tile_blocks<5, S, T, FMT>(sm, a, src, tile); break;
+      case 6: fwd_tile_blocks<6, S, T, FMT>(sm, a, src, tile); break;
+      case 7: fwd_tile_blocks<7, S, T, FMT>(sm, a, src, tile); break;
+      case 8: fwd_tile_blocks<8, S, T, FMT>(sm, a, src, tile); break;
+      case 9: fwd_tile_blocks<9, S, T, FMT>(sm, a, src, tile); break;
+      case 10: fwd_tile_blocks<10, S, T, FMT>(sm, a, src, tile); break;
+      case 11: fwd_tile_blocks<11, S, T, FMT>(sm, a, src, tile); break;
+      case 12: fwd_tile_blocks<12, S, T, FMT>(sm, a, src, tile); break;
+      case 13: fwd_tile_blocks<13, S, T, FMT>(sm, a, src, tile); break;
     }
   } else {
-    const int b = tile >> a.log2R1;
-    const int k1 = tile & (a.R1 - 1);
-    const int shR = a.log2N - a.log2R1, shC = a.log2N - a.log2Nc;
-    const long long p0 = (long long)b * a.hop;
-#pragma unroll 2
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int j1 = 0; j1 < a.R1; ++j1) {
-        const int jj = (j1 << LOGS) + e;
-        float2 z = src.pair(p0 + (CPLX ? jj : 2 * jj));
-        z.x *= a.wscale;
-        z.y *= a.wscale;
-        const int m = (j1 * k1) & (a.R1 - 1);
-        acc = cadd(acc, m == 0 ? z : cmul(z, __ldg(&a.tw_big[m << shR])));
-      }
-      if (k1) acc = cmul(acc, __ldg(&a.tw_big[(e * k1) << shC]));
-      sm[padx(e)] = acc;
-    }
-    __syncthreads();
-    tile_fft<-1, S, T>(sm, a.tw_tile, LOGS);
-    float2* Zb = a.Z + ((size_t)b << a.log2Nc) + ((size_t)k1 << LOGS);
-#pragma unroll 4
-    for (int k = 0; k < E; ++k) {
-      const int e = threadIdx.x + k * T;
-      Zb[e] = sm[padx(e)];
+    switch (a.log2R1) {
+      case 1: fwd_tile_split<1, S, T, FMT>(sm, a, src, tile); break;
+      case 2: fwd_tile_split<2, S, T, FMT>(sm, a, src, tile); break;
+      case 3: fwd_tile_split<3, S, T, FMT>(sm, a, src, tile); break;
     }
   }
 }
 
 // ----------------------------------------------------------------- Welch split
-struct SplitArgs {
-  const float2* Z;
-  float2* X;                   // [B][K]
-  float* P;                    // [B][K] Welch terms
-  int log2N, log2Nc, K, R1, log2R1, logS;
-  const float2* tw_big;        // W_N^k
-};
 
 __device__ __forceinline__ float2 z_at(const SplitArgs& a, const float2* Zb, int m) {
   return __ldg(&Zb[a.R1 == 1 ? m : ((m & (a.R1 - 1)) << a.logS) + (m >> a.log2R1)]);
@@ -222,56 +191,83 @@ __global__ void __launch_bounds__(256) welch_split_kernel(SplitArgs a) {
   }
 }
 
-// ----------------------------------------------------------------- Welch accumulate
-// acc[k] += P[b][k] in block order; every `averages` blocks a record is
-// written (spectrum.rs:116-161) and the accumulator restarts.  fmt: 0 u8,
-// 1 u16 big-endian, 2 f32 mean power.  The u8/u16 arithmetic is rounded per
-// operation (no fused multiply-add) like the reference.
-static __global__ void __launch_bounds__(256) welch_accum_kernel(const float* __restrict__ P, float* acc, int K, int B,
-                                                          int accn0, int averages, int fmt, float db_plus,
-                                                          uint8_t* out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K) return;
-  float s = acc[k];
-  int cnt = accn0, r = 0;
-  for (int b = 0; b < B; ++b) {
-    s += __ldg(&P[(size_t)b * K + k]);
-    if (++cnt >= averages) {
-      const size_t o = (size_t)r * K + k;
-      if (fmt == 2) {
-        reinterpret_cast<float*>(out)[o] = __fdiv_rn(s, (float)cnt);
-      } else {
-        const float db = __fadd_rn(__fmul_rn(log10f(s), 10.0f), db_plus);
-        if (fmt == 1) {
-          const float q = fminf(fmaxf(__fadd_rn(__fmul_rn(db, 20.0f), 4000.0f), 0.0f), 4095.0f);
-          const unsigned v = (unsigned)q;
-          out[2 * o] = (uint8_t)(v >> 8);
-          out[2 * o + 1] = (uint8_t)(v & 0xFF);
-        } else {
-          const float q = fminf(fmaxf(__fadd_rn(__fmul_rn(db, 2.0f), 250.0f), 0.0f), 255.0f);
-          out[o] = (uint8_t)(unsigned)q;
-        }
-      }
-      s = 0.0f;
-      cnt = 0;
-      ++r;
-    }
+// ----------------------------------------------------------------- split + Welch
+// Each warp owns WELCH_WARP_BINS consecutive bins for all B blocks of the
+// buffer: lane l forms X[k0 - 1 + l] (lanes 0 and 31 are the neighbours'
+// halo), takes its neighbours by shuffle, writes X for the filter bank and
+// adds the Hann-by-convolution term |X[k] - (X[k-1]+X[k+1])/2|^2 to the bin's
+// f32 accumulator in block order, exactly as spectrum.rs:90-111 does.  No
+// barrier separates the blocks, so their loads overlap.  Every `averages`
+// blocks a record is written (spectrum.rs:116-161) and the accumulator
+// restarts.  fmt: 0 u8, 1 u16 big-endian, 2 f32 mean power.  The u8/u16
+// arithmetic is rounded per operation (no fused multiply-add) like the
+// reference; only log10f may differ from the host libm in the last place.
+__device__ __forceinline__ void emit_record(const WelchArgs& a, int r, int k, float s, int cnt) {
+  const size_t o = (size_t)r * a.s.K + k;
+  if (a.fmt == 2) {
+    reinterpret_cast<float*>(a.out)[o] = __fdiv_rn(s, (float)cnt);
+    return;
   }
-  acc[k] = s;
+  const float db = __fadd_rn(__fmul_rn(log10f(s), 10.0f), a.db_plus);
+  if (a.fmt == 1) {
+    const float q = fminf(fmaxf(__fadd_rn(__fmul_rn(db, 20.0f), 4000.0f), 0.0f), 4095.0f);
+    const unsigned v = (unsigned)q;
+    a.out[2 * o] = (uint8_t)(v >> 8);
+    a.out[2 * o + 1] = (uint8_t)(v & 0xFF);
+  } else {
+    const float q = fminf(fmaxf(__fadd_rn(__fmul_rn(db, 2.0f), 250.0f), 0.0f), 255.0f);
+    a.out[o] = (uint8_t)(unsigned)q;
+  }
+}
+
+template <bool REAL>
+__global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
+  constexpr int CB = WELCH_WARP_BINS;                        // bins per CTA (every warp covers them)
+  __shared__ float terms[WELCH_CHUNK][CB];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int k0 = blockIdx.x * CB;
+  const int kk = k0 - 1 + lane;                              // bin this lane forms
+  const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
+  const int slot = lane - 1;                                 // owner's column in `terms`
+  const SplitArgs& s = a.s;
+  float2* __restrict__ X = s.X;
+  // Phase B state: thread t sums bin k0 + t.
+  const int kb = k0 + threadIdx.x;
+  const bool summer = threadIdx.x < CB && kb < s.K;
+  float acc = summer ? a.acc[kb] : 0.0f;
+  int cnt = a.accn0, r = 0;
+  for (int b0 = 0; b0 < a.B; b0 += WELCH_CHUNK) {
+    const int nb = min(WELCH_CHUNK, a.B - b0);
+    // Phase A: warp w forms blocks w, w + WARPS, ... (independent loads).
+#pragma unroll 2
+    for (int i = wid; i < nb; i += WELCH_WARPS) {
+      const float2* Zb = s.Z + ((size_t)(b0 + i) << s.log2Nc);
+      const float2 x1 = x_at<REAL>(s, Zb, kk);
+      const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
+      const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
+      if (owner) {
+        X[(size_t)(b0 + i) * s.K + kk] = x1;
+        const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
+        terms[i][slot] = __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
+      }
+    }
+    __syncthreads();
+    // Phase B: accumulate in block order and emit records.
+    for (int i = 0; i < nb; ++i) {
+      if (summer) acc += terms[i][threadIdx.x];
+      if (++cnt >= a.averages) {
+        if (summer) emit_record(a, r, kb, acc, cnt);
+        acc = 0.0f;
+        cnt = 0;
+        ++r;
+      }
+    }
+    __syncthreads();
+  }
+  if (summer) a.acc[kb] = acc;
 }
 
 // ----------------------------------------------------------------- filter bank
-struct FcfbArgs {
-  const TileDesc* tiles;
-  int ntiles;
-  int* cursor;                 // persistent mode: next tile to claim
-  const int2* list;            // (channel, block) per transform
-  const ChanDev* chans;
-  const float2* X;             // [B][K]
-  int K, log2N;
-  const float2* tw;            // W_S^k
-};
-
 template <int S, int T, bool PERSIST, bool REAL>
 __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
   extern __shared__ float2 sm[];
@@ -311,16 +307,6 @@ __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
 // Adjoint of fcfb_kernel.  With g = FFT_n(dy zero-padded to [n/8, 7n/8)) (the
 // forward transform is the adjoint of the unnormalised inverse), v = w * G:
 //   dW[j] += conj(G[j]) g,  dX[bin] += conj(w[j]) g  (conjugated for mirror bins).
-struct BwdArgs {
-  const TileDesc* tiles;
-  const int2* list;
-  const BwdChan* chans;
-  const float2* X;
-  float2* dX;                  // may be null
-  int K, log2N;
-  const float2* tw;
-};
-
 template <int S, int T, bool REAL>
 __global__ void __launch_bounds__(T, 2) fcfb_backward_kernel(BwdArgs a) {
   extern __shared__ float2 sm[];

@@ -33,15 +33,13 @@
 
 #include "spektri_b200.h"
 #include "sk_internal.h"
-#include "sk_kernels.cuh"
+#include "sk_types.h"
 
 using namespace sk;
 
 namespace {
 
 constexpr int S = TILE_S;
-constexpr int T = TILE_T;
-constexpr size_t TILE_SMEM = TileShape<S>::SMEM_BYTES;
 constexpr size_t kScratchElems = SK_NOALLOC_SCRATCH_ELEMS;
 
 static __device__ __align__(256) float2 g_noalloc_scratch[kScratchElems];
@@ -67,27 +65,6 @@ __global__ void noalloc_twiddles(float2* tw_tile, float2* tw_big, int n_big) {
   }
 }
 
-using FwdFn = void (*)(FwdArgs);
-template <int FMT>
-FwdFn fwd_for() { return fwd_fft_kernel<S, T, FMT>; }
-FwdFn fwd_kernel(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S8: return fwd_for<SK_FMT_S8>();
-    case SK_FMT_S16LE: return fwd_for<SK_FMT_S16LE>();
-    case SK_FMT_S16BE: return fwd_for<SK_FMT_S16BE>();
-    case SK_FMT_F32LE: return fwd_for<SK_FMT_F32LE>();
-    case SK_FMT_F32BE: return fwd_for<SK_FMT_F32BE>();
-    case SK_FMT_U8: return fwd_for<SK_FMT_U8>();
-    case SK_FMT_CS8: return fwd_for<SK_FMT_CS8>();
-    case SK_FMT_CS16LE: return fwd_for<SK_FMT_CS16LE>();
-    case SK_FMT_CS16BE: return fwd_for<SK_FMT_CS16BE>();
-    case SK_FMT_CF32LE: return fwd_for<SK_FMT_CF32LE>();
-    case SK_FMT_CF32BE: return fwd_for<SK_FMT_CF32BE>();
-    case SK_FMT_CU8: return fwd_for<SK_FMT_CU8>();
-  }
-  return nullptr;
-}
-
 int log2_exact(long long v) {
   if (v <= 0 || (v & (v - 1))) return -1;
   int r = 0;
@@ -108,7 +85,7 @@ int setup_device(int dev, float2** base) {
     static const int fmts[] = {SK_FMT_S8, SK_FMT_S16LE, SK_FMT_S16BE, SK_FMT_F32LE, SK_FMT_F32BE, SK_FMT_U8,
                                SK_FMT_CS8, SK_FMT_CS16LE, SK_FMT_CS16BE, SK_FMT_CF32LE, SK_FMT_CF32BE, SK_FMT_CU8};
     for (int f : fmts) {
-      e = cudaFuncSetAttribute(fwd_kernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
+      e = fwd_prepare(f);
       if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     }
     d.base = (float2*)p;
@@ -128,9 +105,9 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   const bool cplx = format_complex(input_format);
   const int log2N = log2_exact(fft_size);
   const int log2Nc = log2N - (cplx ? 0 : 1);
-  if (log2N < 3 || log2Nc < 2 || log2Nc > TileShape<S>::LOGS + 3)
+  if (log2N < 3 || log2Nc < 2 || log2Nc > TILE_LOGS + 3)
     return fail(SK_ERR_UNSUPPORTED, "sk_spectra_noalloc: FFT size %u not supported (power of two, 8 .. %d complex points)",
-                fft_size, 1 << (TileShape<S>::LOGS + 3));
+                fft_size, 1 << (TILE_LOGS + 3));
   if ((uintptr_t)raw % (format_bits(input_format) / 8))
     return fail(SK_ERR_ARG, "sk_spectra_noalloc: raw input misaligned for its sample format");
   const long long N = fft_size, Nc = 1ll << log2Nc;
@@ -171,8 +148,8 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   a.log2Nc = log2Nc;
   a.R1 = 1;
   a.log2R1 = 0;
-  if (log2Nc > TileShape<S>::LOGS) {
-    a.log2R1 = log2Nc - TileShape<S>::LOGS;
+  if (log2Nc > TILE_LOGS) {
+    a.log2R1 = log2Nc - TILE_LOGS;
     a.R1 = 1 << a.log2R1;
   }
   a.wscale = format_scaling(input_format) / (float)N;
@@ -186,8 +163,7 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   } else {
     grid = (int)n_blocks * a.R1;
   }
-  fwd_kernel(input_format)<<<grid, T, TILE_SMEM, st>>>(a);
-  e = cudaGetLastError();
+  e = launch_fwd(input_format, grid, a, st);
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "forward FFT kernel: %s", cudaGetErrorString(e));
 
   SplitArgs s{};
@@ -199,12 +175,9 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   s.K = cplx ? (int)N : (int)(N / 2 + 1);
   s.R1 = a.R1;
   s.log2R1 = a.log2R1;
-  s.logS = TileShape<S>::LOGS;
+  s.logS = TILE_LOGS;
   s.tw_big = tw_big;
-  dim3 g2((s.K + 255) / 256, n_blocks);
-  if (cplx) welch_split_kernel<false><<<g2, 256, 0, st>>>(s);
-  else welch_split_kernel<true><<<g2, 256, 0, st>>>(s);
-  e = cudaGetLastError();
+  e = launch_split(cplx, (int)n_blocks, s, st);
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "spectrum split kernel: %s", cudaGetErrorString(e));
   return SK_OK;
 }

@@ -16,15 +16,14 @@
 
 #include "spektri_b200.h"
 #include "sk_internal.h"
-#include "sk_kernels.cuh"
+#include "sk_types.h"
 
 using namespace sk;
 
 namespace {
 
 constexpr int S = TILE_S;
-constexpr int T = TILE_T;
-constexpr size_t TILE_SMEM = TileShape<S>::SMEM_BYTES;
+
 
 int ilog2_exact(long long v) {
   if (v <= 0 || (v & (v - 1))) return -1;
@@ -88,7 +87,6 @@ struct sk_plan {
   int halo_cur = 0;
   float2* d_Z = nullptr;
   float2* d_X = nullptr;
-  float* d_P = nullptr;
   float* d_acc = nullptr;
   float2* d_w = nullptr;
   ChanDev* d_chans = nullptr;
@@ -112,7 +110,7 @@ struct sk_plan {
   // stage timing
   bool timing = false;
   std::vector<std::array<cudaEvent_t, SK_N_STAGES + 1>> ev_pending, ev_free;
-  double stage_ms[SK_N_STAGES] = {0, 0, 0, 0};
+  double stage_ms[SK_N_STAGES] = {};
   uint64_t timed_calls = 0;
 };
 
@@ -121,7 +119,7 @@ namespace {
 int plan_free(sk_plan* pl) {
   if (!pl) return SK_OK;
   DeviceGuard g(pl->p.device);
-  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_X, pl->d_P,
+  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->d_tiles, pl->d_list,
                   pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
   for (void* q : ptrs) if (q) cudaFree(q);
@@ -149,36 +147,9 @@ void twiddles(std::vector<float2>& t, long long n) {
   }
 }
 
-// Kernel instances per input format.
-using FwdFn = void (*)(FwdArgs);
-template <int FMT>
-FwdFn fwd_for() { return fwd_fft_kernel<S, T, FMT>; }
-FwdFn fwd_kernel_for(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S8: return fwd_for<SK_FMT_S8>();
-    case SK_FMT_S16LE: return fwd_for<SK_FMT_S16LE>();
-    case SK_FMT_S16BE: return fwd_for<SK_FMT_S16BE>();
-    case SK_FMT_F32LE: return fwd_for<SK_FMT_F32LE>();
-    case SK_FMT_F32BE: return fwd_for<SK_FMT_F32BE>();
-    case SK_FMT_U8: return fwd_for<SK_FMT_U8>();
-    case SK_FMT_CS8: return fwd_for<SK_FMT_CS8>();
-    case SK_FMT_CS16LE: return fwd_for<SK_FMT_CS16LE>();
-    case SK_FMT_CS16BE: return fwd_for<SK_FMT_CS16BE>();
-    case SK_FMT_CF32LE: return fwd_for<SK_FMT_CF32LE>();
-    case SK_FMT_CF32BE: return fwd_for<SK_FMT_CF32BE>();
-    case SK_FMT_CU8: return fwd_for<SK_FMT_CU8>();
-  }
-  return nullptr;
-}
-
-int set_smem_attrs(FwdFn f) {
-  SK_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_kernel<S, T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_backward_kernel<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
-  SK_CUDA(cudaFuncSetAttribute(fcfb_backward_kernel<S, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM));
+int set_smem_attrs(int fmt) {
+  SK_CUDA(fwd_prepare(fmt));
+  SK_CUDA(fcfb_prepare());
   return SK_OK;
 }
 
@@ -197,7 +168,14 @@ std::array<cudaEvent_t, SK_N_STAGES + 1>* timing_events(sk_plan* pl) {
   return &pl->ev_pending.back();
 }
 
-int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, float* P, cudaStream_t st,
+// Forward FFTs of one buffer, then either the spectrum split alone (welch ==
+// nullptr) or the split fused with the Welch accumulation and its records.
+struct WelchCall {
+  int accn0;
+  uint8_t* out;
+};
+
+int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
                    std::array<cudaEvent_t, SK_N_STAGES + 1>* ev = nullptr) {
   FwdArgs a{};
   a.raw = raw;
@@ -223,24 +201,33 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, float* P, cudaStr
     grid = pl->B * pl->R1;
   }
   if (ev) SK_CUDA(cudaEventRecord((*ev)[0], st));
-  fwd_kernel_for(pl->fmt)<<<grid, T, TILE_SMEM, st>>>(a);
-  SK_CUDA(cudaGetLastError());
+  SK_CUDA(launch_fwd(pl->fmt, grid, a, st));
   if (ev) SK_CUDA(cudaEventRecord((*ev)[1], st));
   SplitArgs s{};
   s.Z = pl->d_Z;
   s.X = X;
-  s.P = P;
+  s.P = nullptr;
   s.log2N = pl->log2N;
   s.log2Nc = pl->log2Nc;
   s.K = pl->K;
   s.R1 = pl->R1;
   s.log2R1 = pl->log2R1;
-  s.logS = TileShape<S>::LOGS;
+  s.logS = TILE_LOGS;
   s.tw_big = pl->d_tw_big;
-  dim3 g2((pl->K + 255) / 256, pl->B);
-  if (pl->cplx) welch_split_kernel<false><<<g2, 256, 0, st>>>(s);
-  else welch_split_kernel<true><<<g2, 256, 0, st>>>(s);
-  SK_CUDA(cudaGetLastError());
+  if (welch) {
+    WelchArgs w{};
+    w.s = s;
+    w.acc = pl->d_acc;
+    w.B = pl->B;
+    w.accn0 = welch->accn0;
+    w.averages = pl->averages;
+    w.fmt = pl->spec_fmt;
+    w.db_plus = pl->db_plus;
+    w.out = welch->out;
+    SK_CUDA(launch_welch(pl->cplx, w, st));
+  } else {
+    SK_CUDA(launch_split(pl->cplx, pl->B, s, st));
+  }
   if (ev) SK_CUDA(cudaEventRecord((*ev)[2], st));
   pl->halo_cur ^= 1;
   return SK_OK;
@@ -260,21 +247,16 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
   return a;
 }
 
-int launch_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
+int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, chans, X);
   if (batched) {
     SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
     const int grid = std::min(pl->persist_grid, pl->n_batched_tiles);
-    if (pl->cplx) fcfb_kernel<S, T, true, false><<<grid, T, TILE_SMEM, st>>>(a, 0);
-    else fcfb_kernel<S, T, true, true><<<grid, T, TILE_SMEM, st>>>(a, 0);
-    SK_CUDA(cudaGetLastError());
+    SK_CUDA(launch_fcfb(pl->cplx, true, grid, a, 0, st));
   } else {
-    for (size_t c = 0; c < pl->ch.size(); ++c) {
-      if (pl->cplx) fcfb_kernel<S, T, false, false><<<pl->plain_count[c], T, TILE_SMEM, st>>>(a, pl->plain_start[c]);
-      else fcfb_kernel<S, T, false, true><<<pl->plain_count[c], T, TILE_SMEM, st>>>(a, pl->plain_start[c]);
-      SK_CUDA(cudaGetLastError());
-    }
+    for (size_t c = 0; c < pl->ch.size(); ++c)
+      SK_CUDA(launch_fcfb(pl->cplx, false, pl->plain_count[c], a, pl->plain_start[c], st));
   }
   return SK_OK;
 }
@@ -304,7 +286,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   const int log2N = ilog2_exact(p.fft_size);
   const int log2Nc = log2N - (cplx ? 0 : 1);
   if (log2N < 0 || log2Nc < 2 || log2N < 3) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path needs a power of two >= 8", p.fft_size);
-  const int maxLogNc = TileShape<S>::LOGS + 3;   // R1 <= 8
+  const int maxLogNc = TILE_LOGS + 3;   // R1 <= 8
   if (log2Nc > maxLogNc) return fail(SK_ERR_UNSUPPORTED, "FFT size %u exceeds the device limit (complex length %d)", p.fft_size, 1 << maxLogNc);
 
   sk_plan* pl = new sk_plan();
@@ -320,8 +302,8 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   pl->K = cplx ? (int)pl->N : (int)(pl->N / 2 + 1);
   pl->log2N = log2N;
   pl->log2Nc = log2Nc;
-  if (log2Nc > TileShape<S>::LOGS) {
-    pl->log2R1 = log2Nc - TileShape<S>::LOGS;
+  if (log2Nc > TILE_LOGS) {
+    pl->log2R1 = log2Nc - TILE_LOGS;
     pl->R1 = 1 << pl->log2R1;
   }
   pl->wscale = format_scaling(p.input_format) / (float)pl->N;      // dsp.rs:70-73
@@ -342,7 +324,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       fprintf(stderr, "Invalid filter parameters\n");
     } else {
       const int l2 = ilog2_exact(bins);
-      if (l2 < 2 || l2 > TileShape<S>::LOGS) {
+      if (l2 < 2 || l2 > TILE_LOGS) {
         st = SK_ERR_UNSUPPORTED;
         fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two 4..%d)\n", bins, S);
       } else {
@@ -379,7 +361,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   if (!g.ok) { plan_free(pl); return fail(SK_ERR_CUDA, "cudaSetDevice(%d) failed", p.device); }
   int rc = SK_OK;
 #define TRY(x) do { rc = (x); if (rc != SK_OK) { plan_free(pl); return rc; } } while (0)
-  TRY(set_smem_attrs(fwd_kernel_for(pl->fmt)));
+  TRY(set_smem_attrs(pl->fmt));
   {
     cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { plan_free(pl); return fail(SK_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
@@ -394,7 +376,6 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
   TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
   TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->K));
-  TRY(dev_alloc(&pl->d_P, (size_t)pl->B * pl->K));
   TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
   TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
   TRY(dev_alloc(&pl->d_chans, pl->ch.size()));
@@ -433,7 +414,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   // channel's own tiles.
   std::vector<int2> list;
   std::vector<TileDesc> tiles;
-  for (int l2 = TileShape<S>::LOGS; l2 >= 2; --l2) {
+  for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
     const int per = std::min(S >> l2, MAX_TILE_TRANSFORMS);
     const int base = (int)list.size();
     for (size_t c = 0; c < pl->ch.size(); ++c)
@@ -457,7 +438,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   if (!tiles.empty()) CUDA_TRY(cudaMemcpy(pl->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
   int sms = 0, per_sm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcfb_kernel<S, T, true, true>, T, TILE_SMEM));
+  CUDA_TRY(fcfb_occupancy(&per_sm));
   pl->persist_grid = std::max(1, sms * std::max(1, per_sm));
 #undef TRY
 #undef CUDA_TRY
@@ -503,7 +484,7 @@ int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
 int sk_launches_per_call(const sk_plan* pl) {
   if (!pl) return fail(SK_ERR_ARG, "null plan");
   const int fb = pl->ch.empty() ? 0 : (pl->p.mode == SK_MODE_BATCHED ? 1 : (int)pl->ch.size());
-  return 3 + fb;
+  return 2 + fb;
 }
 
 int sk_set_weights(sk_plan* pl, int32_t c, const float* w) {
@@ -554,15 +535,12 @@ int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void*
   const uint32_t n_spec = total / (uint32_t)pl->averages;
   if (n_spec > 0 && !spec_out) return fail(SK_ERR_ARG, "spectrum records complete in this call but spec_out is null");
   auto* ev = timing_events(pl);
-  int rc = launch_forward(pl, (const uint8_t*)raw, pl->d_X, pl->d_P, st, ev);
+  const WelchCall wc{(int)pl->accn, (uint8_t*)spec_out};
+  int rc = launch_forward(pl, (const uint8_t*)raw, pl->d_X, &wc, st, ev);
   if (rc) return rc;
-  welch_accum_kernel<<<(pl->K + 255) / 256, 256, 0, st>>>(pl->d_P, pl->d_acc, pl->K, pl->B, (int)pl->accn,
-                                                          pl->averages, pl->spec_fmt, pl->db_plus, (uint8_t*)spec_out);
-  SK_CUDA(cudaGetLastError());
+  rc = run_fcfb(pl, pl->d_chans, pl->d_X, pl->p.mode == SK_MODE_BATCHED, st);
+  if (rc) return rc;
   if (ev) SK_CUDA(cudaEventRecord((*ev)[3], st));
-  rc = launch_fcfb(pl, pl->d_chans, pl->d_X, pl->p.mode == SK_MODE_BATCHED, st);
-  if (rc) return rc;
-  if (ev) SK_CUDA(cudaEventRecord((*ev)[4], st));
   if (result) {
     result->n_spectra = n_spec;
     result->reserved = 0;
@@ -632,8 +610,7 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   }
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
-  if (pl->cplx) fcfb_kernel<S, T, false, false><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a, 0);
-  else fcfb_kernel<S, T, false, true><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a, 0);
+  SK_CUDA(launch_fcfb(pl->cplx, false, pl->n_batched_tiles, a, 0, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
@@ -666,8 +643,7 @@ int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, 
   a.K = pl->K;
   a.log2N = pl->log2N;
   a.tw = pl->d_tw_tile;
-  if (pl->cplx) fcfb_backward_kernel<S, T, false><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a);
-  else fcfb_backward_kernel<S, T, true><<<pl->n_batched_tiles, T, TILE_SMEM, st>>>(a);
+  SK_CUDA(launch_fcfb_backward(pl->cplx, pl->n_batched_tiles, a, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }

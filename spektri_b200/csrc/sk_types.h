@@ -1,0 +1,110 @@
+// Kernel argument structures, tile constants and the launchers that the host
+// code calls.  Host-compilable: the kernels themselves live in the .cu files
+// that include sk_kernels.cuh (one instantiation each).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sk {
+
+constexpr int TILE_S = 8192;              // complex elements per FFT tile
+constexpr int TILE_T = 256;               // threads per tile CTA (32 elements each)
+constexpr int TILE_LOGS = 13;
+constexpr int MAX_TILE_TRANSFORMS = 256;  // transforms per filter-bank tile
+// Tile in shared memory: S complex values with one pad slot per 16.
+constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
+constexpr int WELCH_WARP_BINS = 30;       // bins per Welch CTA (a warp plus a 1-bin halo each side)
+constexpr int WELCH_WARPS = 8;            // warps per Welch CTA (they split the blocks)
+constexpr int WELCH_CHUNK = 64;           // blocks whose Welch terms a CTA stages at once
+
+struct ChanDev {               // one filter-bank channel, as the kernels see it
+  const float2* w;             // weights, natural order: w[j] scales bin first+j
+  float2* out;                 // B * 6(n/8) outputs
+  long long first;
+  int log2n;
+  int pad;
+};
+struct BwdChan {
+  const float2* w;
+  const float2* dy;            // B * 6(n/8) output gradients
+  float2* dw;                  // n weight gradients (accumulated)
+  long long first;
+  int log2n;
+  int pad;
+};
+struct TileDesc {              // transforms of one size
+  int log2n;
+  int list_off;                // first entry in the (channel, block) list
+  int count;                   // transforms in this tile
+  int pad;
+};
+
+struct FwdArgs {
+  const uint8_t* raw;          // new samples of this buffer
+  const float* halo;           // converted last N/4 samples of the previous buffer
+  float* halo_next;            // receives the converted last N/4 samples of this one
+  long long overlap, nnew;
+  int hop, B;
+  int log2N, log2Nc;           // N (window length) and Nc (complex FFT length)
+  int R1, log2R1;              // Nc = R1 * S when Nc > S (R1 = 1 otherwise)
+  float wscale;                // rectangular window value scaling/N (dsp.rs:70-73)
+  const float2* tw_tile;       // W_S^k
+  const float2* tw_big;        // W_N^k, k < N
+  float2* Z;                   // [B][Nc]; for R1 > 1 element k1 + R1*k2 sits at k1*S + k2
+};
+
+struct SplitArgs {
+  const float2* Z;
+  float2* X;                   // [B][K]
+  float* P;                    // [B][K] Welch terms (may be null)
+  int log2N, log2Nc, K, R1, log2R1, logS;
+  const float2* tw_big;        // W_N^k
+};
+
+struct WelchArgs {
+  SplitArgs s;                 // Z -> X (P unused)
+  float* acc;                  // [K] running accumulator (carried across buffers)
+  int B, accn0, averages, fmt;
+  float db_plus;               // -10 log10(averages), computed on the host in f32
+  uint8_t* out;                // records, K bins each
+};
+
+struct FcfbArgs {
+  const TileDesc* tiles;
+  int ntiles;
+  int* cursor;                 // persistent mode: next tile to claim
+  const int2* list;            // (channel, block) per transform
+  const ChanDev* chans;
+  const float2* X;             // [B][K]
+  int K, log2N;
+  const float2* tw;            // W_S^k
+};
+
+struct BwdArgs {
+  const TileDesc* tiles;
+  const int2* list;
+  const BwdChan* chans;
+  const float2* X;
+  float2* dX;                  // may be null
+  int K, log2N;
+  const float2* tw;
+};
+
+// Launchers (sk_fwd_*.cu, sk_kern.cu).  Each returns the launch status.
+cudaError_t fwd_prepare(int fmt);                         // shared-memory limit of the format's kernel
+cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
+cudaError_t fwd_prepare_8(int fmt);
+cudaError_t fwd_prepare_16(int fmt);
+cudaError_t fwd_prepare_32(int fmt);
+cudaError_t launch_fwd_8(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
+cudaError_t launch_fwd_16(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
+cudaError_t launch_fwd_32(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
+cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
+cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st);
+cudaError_t fcfb_prepare();
+cudaError_t fcfb_occupancy(int* ctas_per_sm);
+cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st);
+cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
+
+}  // namespace sk

@@ -201,8 +201,8 @@ class Plan:
         check(lib().sk_plan_set_timing(self._h, int(bool(enable))))
 
     def timing(self):
-        """(ms per stage [fwd_fft, welch_split, welch_accum, fcfb], calls) since the last read."""
-        ms = (C.c_double * 4)()
+        """(ms per stage [fwd_fft, welch, fcfb], calls) since the last read."""
+        ms = (C.c_double * 3)()
         n = C.c_uint64()
         check(lib().sk_plan_timing(self._h, ms, C.byref(n)), "sk_plan_timing")
         return list(ms), n.value
