@@ -23,4 +23,14 @@ cudaError_t launch_fwd_16(int fmt, int grid, const FwdArgs& a, cudaStream_t st) 
   return cudaErrorInvalidValue;
 }
 
+const void* fwd_kernel_ptr_16(int fmt) {
+  switch (fmt) {
+    case SK_FMT_S16LE: return fwd_ptr_one<SK_FMT_S16LE>();
+    case SK_FMT_S16BE: return fwd_ptr_one<SK_FMT_S16BE>();
+    case SK_FMT_CS16LE: return fwd_ptr_one<SK_FMT_CS16LE>();
+    case SK_FMT_CS16BE: return fwd_ptr_one<SK_FMT_CS16BE>();
+  }
+  return nullptr;
+}
+
 }  // namespace sk

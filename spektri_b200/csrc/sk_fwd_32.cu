@@ -23,4 +23,14 @@ cudaError_t launch_fwd_32(int fmt, int grid, const FwdArgs& a, cudaStream_t st) 
   return cudaErrorInvalidValue;
 }
 
+const void* fwd_kernel_ptr_32(int fmt) {
+  switch (fmt) {
+    case SK_FMT_F32LE: return fwd_ptr_one<SK_FMT_F32LE>();
+    case SK_FMT_F32BE: return fwd_ptr_one<SK_FMT_F32BE>();
+    case SK_FMT_CF32LE: return fwd_ptr_one<SK_FMT_CF32LE>();
+    case SK_FMT_CF32BE: return fwd_ptr_one<SK_FMT_CF32BE>();
+  }
+  return nullptr;
+}
+
 }  // namespace sk

@@ -23,4 +23,14 @@ cudaError_t launch_fwd_8(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
+const void* fwd_kernel_ptr_8(int fmt) {
+  switch (fmt) {
+    case SK_FMT_S8: return fwd_ptr_one<SK_FMT_S8>();
+    case SK_FMT_U8: return fwd_ptr_one<SK_FMT_U8>();
+    case SK_FMT_CS8: return fwd_ptr_one<SK_FMT_CS8>();
+    case SK_FMT_CU8: return fwd_ptr_one<SK_FMT_CU8>();
+  }
+  return nullptr;
+}
+
 }  // namespace sk

@@ -19,4 +19,9 @@ cudaError_t fwd_prepare_one() {
                               (int)TILE_SMEM);
 }
 
+template <int FMT>
+const void* fwd_ptr_one() {
+  return (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
+}
+
 }  // namespace sk

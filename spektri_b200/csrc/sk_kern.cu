@@ -24,6 +24,19 @@ cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
+const void* fwd_kernel_ptr(int fmt) {
+  switch (format_bits(fmt)) {
+    case 8: return fwd_kernel_ptr_8(fmt);
+    case 16: return fwd_kernel_ptr_16(fmt);
+    case 32: return fwd_kernel_ptr_32(fmt);
+  }
+  return nullptr;
+}
+
+const void* welch_kernel_ptr(bool cplx) {
+  return cplx ? (const void*)welch_kernel<false> : (const void*)welch_kernel<true>;
+}
+
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) {
   const dim3 g((s.K + 255) / 256, B);
   if (cplx) welch_split_kernel<false><<<g, 256, 0, st>>>(s);

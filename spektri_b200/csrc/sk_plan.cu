@@ -107,6 +107,12 @@ struct sk_plan {
   uint8_t* d_spec = nullptr;
   size_t out_total = 0;
   std::vector<void*> d_out_ptrs;
+  // batched mode: one call's work captured once and replayed from a CUDA
+  // graph; per call only the forward and Welch kernel arguments change.
+  cudaGraph_t graph = nullptr;          // kept: its nodes address the executable's nodes
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphNode_t node_fwd = nullptr, node_welch = nullptr;
+  cudaKernelNodeParams p_fwd{}, p_welch{};
   // stage timing
   bool timing = false;
   std::vector<std::array<cudaEvent_t, SK_N_STAGES + 1>> ev_pending, ev_free;
@@ -122,6 +128,8 @@ int plan_free(sk_plan* pl) {
   void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->d_tiles, pl->d_list,
                   pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
+  if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
+  if (pl->graph) cudaGraphDestroy(pl->graph);
   for (void* q : ptrs) if (q) cudaFree(q);
   for (auto* v : {&pl->ev_pending, &pl->ev_free})
     for (auto& a : *v)
@@ -175,8 +183,7 @@ struct WelchCall {
   uint8_t* out;
 };
 
-int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
-                   std::array<cudaEvent_t, SK_N_STAGES + 1>* ev = nullptr) {
+FwdArgs fwd_args(const sk_plan* pl, const uint8_t* raw) {
   FwdArgs a{};
   a.raw = raw;
   a.halo = pl->d_halo[pl->halo_cur];
@@ -193,16 +200,18 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* 
   a.tw_tile = pl->d_tw_tile;
   a.tw_big = pl->d_tw_big;
   a.Z = pl->d_Z;
-  int grid;
+  return a;
+}
+
+int fwd_grid(const sk_plan* pl) {
   if (pl->R1 == 1) {
     const int per = S >> pl->log2Nc;
-    grid = (pl->B + per - 1) / per;
-  } else {
-    grid = pl->B * pl->R1;
+    return (pl->B + per - 1) / per;
   }
-  if (ev) SK_CUDA(cudaEventRecord((*ev)[0], st));
-  SK_CUDA(launch_fwd(pl->fmt, grid, a, st));
-  if (ev) SK_CUDA(cudaEventRecord((*ev)[1], st));
+  return pl->B * pl->R1;
+}
+
+SplitArgs split_args(const sk_plan* pl, float2* X) {
   SplitArgs s{};
   s.Z = pl->d_Z;
   s.X = X;
@@ -214,20 +223,29 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* 
   s.log2R1 = pl->log2R1;
   s.logS = TILE_LOGS;
   s.tw_big = pl->d_tw_big;
-  if (welch) {
-    WelchArgs w{};
-    w.s = s;
-    w.acc = pl->d_acc;
-    w.B = pl->B;
-    w.accn0 = welch->accn0;
-    w.averages = pl->averages;
-    w.fmt = pl->spec_fmt;
-    w.db_plus = pl->db_plus;
-    w.out = welch->out;
-    SK_CUDA(launch_welch(pl->cplx, w, st));
-  } else {
-    SK_CUDA(launch_split(pl->cplx, pl->B, s, st));
-  }
+  return s;
+}
+
+WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
+  WelchArgs w{};
+  w.s = split_args(pl, X);
+  w.acc = pl->d_acc;
+  w.B = pl->B;
+  w.accn0 = c.accn0;
+  w.averages = pl->averages;
+  w.fmt = pl->spec_fmt;
+  w.db_plus = pl->db_plus;
+  w.out = c.out;
+  return w;
+}
+
+int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
+                   std::array<cudaEvent_t, SK_N_STAGES + 1>* ev = nullptr) {
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[0], st));
+  SK_CUDA(launch_fwd(pl->fmt, fwd_grid(pl), fwd_args(pl, raw), st));
+  if (ev) SK_CUDA(cudaEventRecord((*ev)[1], st));
+  if (welch) SK_CUDA(launch_welch(pl->cplx, welch_args(pl, X, *welch), st));
+  else SK_CUDA(launch_split(pl->cplx, pl->B, split_args(pl, X), st));
   if (ev) SK_CUDA(cudaEventRecord((*ev)[2], st));
   pl->halo_cur ^= 1;
   return SK_OK;
@@ -258,6 +276,66 @@ int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, c
     for (size_t c = 0; c < pl->ch.size(); ++c)
       SK_CUDA(launch_fcfb(pl->cplx, false, pl->plain_count[c], a, pl->plain_start[c], st));
   }
+  return SK_OK;
+}
+
+// Batched call through the plan's CUDA graph: [forward FFT] -> [split +
+// Welch] -> [cursor reset] -> [persistent filter bank].  The first call
+// captures it on the plan's stream; later calls patch the two kernel nodes
+// whose arguments change (input pointer and carry buffers; Welch state and
+// record buffer) and replay it on `st`.
+int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t st) {
+  const FwdArgs fa = fwd_args(pl, raw);
+  const WelchArgs wa = welch_args(pl, pl->d_X, wc);
+  if (!pl->graph_exec) {
+    SK_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t e1 = launch_fwd(pl->fmt, fwd_grid(pl), fa, pl->stream);
+    const cudaError_t e2 = launch_welch(pl->cplx, wa, pl->stream);
+    const int rc = run_fcfb(pl, pl->d_chans, pl->d_X, true, pl->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e3 = cudaStreamEndCapture(pl->stream, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || rc != SK_OK || e3 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(SK_ERR_CUDA, "capturing the batched graph failed: %s / %s / %s", cudaGetErrorString(e1),
+                  cudaGetErrorString(e2), cudaGetErrorString(e3));
+    }
+    size_t n = 0;
+    cudaGraphGetNodes(g, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    cudaGraphGetNodes(g, nodes.data(), &n);
+    const void* f_fwd = fwd_kernel_ptr(pl->fmt);
+    const void* f_welch = welch_kernel_ptr(pl->cplx);
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams kp{};
+      if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) continue;
+      if (kp.func == f_fwd) { pl->node_fwd = nd; pl->p_fwd = kp; }
+      if (kp.func == f_welch) { pl->node_welch = nd; pl->p_welch = kp; }
+    }
+    const cudaError_t e4 = (pl->node_fwd && pl->node_welch) ? cudaGraphInstantiate(&pl->graph_exec, g, 0)
+                                                            : cudaErrorInvalidValue;
+    if (e4 != cudaSuccess) {
+      cudaGraphDestroy(g);
+      pl->graph_exec = nullptr;
+      pl->node_fwd = pl->node_welch = nullptr;
+      return fail(SK_ERR_CUDA, "instantiating the batched graph failed: %s", cudaGetErrorString(e4));
+    }
+    pl->graph = g;
+  } else {
+    cudaKernelNodeParams p = pl->p_fwd;
+    void* a1[] = {(void*)&fa};
+    p.kernelParams = a1;
+    p.extra = nullptr;
+    SK_CUDA(cudaGraphExecKernelNodeSetParams(pl->graph_exec, pl->node_fwd, &p));
+    cudaKernelNodeParams q = pl->p_welch;
+    void* a2[] = {(void*)&wa};
+    q.kernelParams = a2;
+    q.extra = nullptr;
+    SK_CUDA(cudaGraphExecKernelNodeSetParams(pl->graph_exec, pl->node_welch, &q));
+  }
+  SK_CUDA(cudaGraphLaunch(pl->graph_exec, st));
+  pl->halo_cur ^= 1;
   return SK_OK;
 }
 
@@ -534,13 +612,19 @@ int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void*
   const uint32_t total = pl->accn + (uint32_t)pl->B;
   const uint32_t n_spec = total / (uint32_t)pl->averages;
   if (n_spec > 0 && !spec_out) return fail(SK_ERR_ARG, "spectrum records complete in this call but spec_out is null");
-  auto* ev = timing_events(pl);
   const WelchCall wc{(int)pl->accn, (uint8_t*)spec_out};
-  int rc = launch_forward(pl, (const uint8_t*)raw, pl->d_X, &wc, st, ev);
-  if (rc) return rc;
-  rc = run_fcfb(pl, pl->d_chans, pl->d_X, pl->p.mode == SK_MODE_BATCHED, st);
-  if (rc) return rc;
-  if (ev) SK_CUDA(cudaEventRecord((*ev)[3], st));
+  int rc;
+  if (pl->p.mode == SK_MODE_BATCHED && !pl->timing && !pl->ch.empty()) {
+    rc = run_graph(pl, (const uint8_t*)raw, wc, st);
+    if (rc) return rc;
+  } else {
+    auto* ev = timing_events(pl);
+    rc = launch_forward(pl, (const uint8_t*)raw, pl->d_X, &wc, st, ev);
+    if (rc) return rc;
+    rc = run_fcfb(pl, pl->d_chans, pl->d_X, pl->p.mode == SK_MODE_BATCHED, st);
+    if (rc) return rc;
+    if (ev) SK_CUDA(cudaEventRecord((*ev)[3], st));
+  }
   if (result) {
     result->n_spectra = n_spec;
     result->reserved = 0;

@@ -106,5 +106,11 @@ cudaError_t fcfb_prepare();
 cudaError_t fcfb_occupancy(int* ctas_per_sm);
 cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
+// Kernel entry addresses (to recognise the nodes of a captured graph).
+const void* fwd_kernel_ptr(int fmt);
+const void* fwd_kernel_ptr_8(int fmt);
+const void* fwd_kernel_ptr_16(int fmt);
+const void* fwd_kernel_ptr_32(int fmt);
+const void* welch_kernel_ptr(bool cplx);
 
 }  // namespace sk
