@@ -188,6 +188,10 @@ int sk_launches_per_call(const sk_plan* plan);
  *                       torch's convention for real losses of complex tensors
  *                       (dL/d conj(z)). */
 int sk_spectra_device(sk_plan* plan, const void* raw, float* X, void* stream);
+/* Stateless variant: raw holds the whole window, overlap + new samples
+ * (N/4 + 3N/4 * B), so the same window always gives the same spectra and the
+ * plan's carry is untouched; used to recompute spectra in backward passes. */
+int sk_spectra_window_device(sk_plan* plan, const void* raw_window, float* X, void* stream);
 int sk_fcfb_forward_device(sk_plan* plan, const float* X, const float* const* W, float* const* y, void* stream);
 int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W, const float* const* dy,
                             float* const* dW, float* dX, void* stream);

@@ -87,6 +87,7 @@ PROTOTYPES = [
     ("sk_synchronize", C.c_int, [C.c_void_p]),
     ("sk_launches_per_call", C.c_int, [C.c_void_p]),
     ("sk_spectra_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("sk_spectra_window_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sk_fcfb_forward_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sk_fcfb_backward_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p]),

@@ -677,6 +677,22 @@ int sk_spectra_device(sk_plan* pl, const void* raw, float* X, void* stream) {
   return launch_forward(pl, (const uint8_t*)raw, (float2*)X, nullptr, st);
 }
 
+int sk_spectra_window_device(sk_plan* pl, const void* raw_window, float* X, void* stream) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (!raw_window || !X) return fail(SK_ERR_ARG, "null argument");
+  if ((uintptr_t)raw_window % (format_bits(pl->fmt) / 8)) return fail(SK_ERR_ARG, "raw window misaligned");
+  DeviceGuard g(pl->p.device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  FwdArgs a = fwd_args(pl, (const uint8_t*)raw_window);
+  a.halo = nullptr;             // every sample, the first N/4 included, comes from the window
+  a.halo_next = nullptr;
+  a.overlap = 0;
+  a.nnew = pl->total;
+  SK_CUDA(launch_fwd(pl->fmt, fwd_grid(pl), a, st));
+  SK_CUDA(launch_split(pl->cplx, pl->B, split_args(pl, (float2*)X), st));
+  return SK_OK;
+}
+
 int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, float* const* y, void* stream) {
   if (check_plan(pl)) return SK_ERR_ARG;
   if (!X || (!pl->ch.empty() && (!W || !y))) return fail(SK_ERR_ARG, "null argument");

@@ -215,6 +215,11 @@ class Plan:
         stream = _stream(stream, self.device)
         check(lib().sk_spectra_device(self._h, _ptr(raw), _ptr(X), stream), "sk_spectra_device")
 
+    def spectra_window_device(self, raw_window, X, stream=None):
+        """Stateless spectra of a window of N/4 + new samples (carry untouched)."""
+        stream = _stream(stream, self.device)
+        check(lib().sk_spectra_window_device(self._h, _ptr(raw_window), _ptr(X), stream), "sk_spectra_window_device")
+
     def fcfb_forward_device(self, X, W, y, stream=None):
         stream = _stream(stream, self.device)
         wt = (C.c_void_p * max(1, len(W)))(*[_ptr(w) for w in W])
