@@ -3,33 +3,33 @@
 
 namespace sk {
 
+#define SK_FOR_FORMATS(X) X(SK_FMT_S16LE) X(SK_FMT_S16BE) X(SK_FMT_CS16LE) X(SK_FMT_CS16BE)
+
 cudaError_t fwd_prepare_16(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S16LE: return fwd_prepare_one<SK_FMT_S16LE>();
-    case SK_FMT_S16BE: return fwd_prepare_one<SK_FMT_S16BE>();
-    case SK_FMT_CS16LE: return fwd_prepare_one<SK_FMT_CS16LE>();
-    case SK_FMT_CS16BE: return fwd_prepare_one<SK_FMT_CS16BE>();
-  }
+#define CASE(F) case F: return fwd_prepare_one<F>();
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_fwd_16(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
-  switch (fmt) {
-    case SK_FMT_S16LE: return fwd_launch_one<SK_FMT_S16LE>(grid, a, st);
-    case SK_FMT_S16BE: return fwd_launch_one<SK_FMT_S16BE>(grid, a, st);
-    case SK_FMT_CS16LE: return fwd_launch_one<SK_FMT_CS16LE>(grid, a, st);
-    case SK_FMT_CS16BE: return fwd_launch_one<SK_FMT_CS16BE>(grid, a, st);
-  }
+#define CASE(F) case F: return fwd_launch_one<F>(grid, a, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr_16(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S16LE: return fwd_ptr_one<SK_FMT_S16LE>();
-    case SK_FMT_S16BE: return fwd_ptr_one<SK_FMT_S16BE>();
-    case SK_FMT_CS16LE: return fwd_ptr_one<SK_FMT_CS16LE>();
-    case SK_FMT_CS16BE: return fwd_ptr_one<SK_FMT_CS16BE>();
-  }
+cudaError_t launch_fwd_col_16(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
+#define CASE(F) case F: return fwd_col_launch_one<F>(grid, a, Y, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
+  return cudaErrorInvalidValue;
+}
+
+const void* fwd_kernel_ptr_16(int fmt, bool col) {
+#define CASE(F) case F: return fwd_ptr_one<F>(col);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return nullptr;
 }
 

@@ -3,33 +3,33 @@
 
 namespace sk {
 
+#define SK_FOR_FORMATS(X) X(SK_FMT_F32LE) X(SK_FMT_F32BE) X(SK_FMT_CF32LE) X(SK_FMT_CF32BE)
+
 cudaError_t fwd_prepare_32(int fmt) {
-  switch (fmt) {
-    case SK_FMT_F32LE: return fwd_prepare_one<SK_FMT_F32LE>();
-    case SK_FMT_F32BE: return fwd_prepare_one<SK_FMT_F32BE>();
-    case SK_FMT_CF32LE: return fwd_prepare_one<SK_FMT_CF32LE>();
-    case SK_FMT_CF32BE: return fwd_prepare_one<SK_FMT_CF32BE>();
-  }
+#define CASE(F) case F: return fwd_prepare_one<F>();
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_fwd_32(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
-  switch (fmt) {
-    case SK_FMT_F32LE: return fwd_launch_one<SK_FMT_F32LE>(grid, a, st);
-    case SK_FMT_F32BE: return fwd_launch_one<SK_FMT_F32BE>(grid, a, st);
-    case SK_FMT_CF32LE: return fwd_launch_one<SK_FMT_CF32LE>(grid, a, st);
-    case SK_FMT_CF32BE: return fwd_launch_one<SK_FMT_CF32BE>(grid, a, st);
-  }
+#define CASE(F) case F: return fwd_launch_one<F>(grid, a, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr_32(int fmt) {
-  switch (fmt) {
-    case SK_FMT_F32LE: return fwd_ptr_one<SK_FMT_F32LE>();
-    case SK_FMT_F32BE: return fwd_ptr_one<SK_FMT_F32BE>();
-    case SK_FMT_CF32LE: return fwd_ptr_one<SK_FMT_CF32LE>();
-    case SK_FMT_CF32BE: return fwd_ptr_one<SK_FMT_CF32BE>();
-  }
+cudaError_t launch_fwd_col_32(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
+#define CASE(F) case F: return fwd_col_launch_one<F>(grid, a, Y, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
+  return cudaErrorInvalidValue;
+}
+
+const void* fwd_kernel_ptr_32(int fmt, bool col) {
+#define CASE(F) case F: return fwd_ptr_one<F>(col);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return nullptr;
 }
 

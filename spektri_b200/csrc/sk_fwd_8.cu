@@ -3,33 +3,33 @@
 
 namespace sk {
 
+#define SK_FOR_FORMATS(X) X(SK_FMT_S8) X(SK_FMT_U8) X(SK_FMT_CS8) X(SK_FMT_CU8)
+
 cudaError_t fwd_prepare_8(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S8: return fwd_prepare_one<SK_FMT_S8>();
-    case SK_FMT_U8: return fwd_prepare_one<SK_FMT_U8>();
-    case SK_FMT_CS8: return fwd_prepare_one<SK_FMT_CS8>();
-    case SK_FMT_CU8: return fwd_prepare_one<SK_FMT_CU8>();
-  }
+#define CASE(F) case F: return fwd_prepare_one<F>();
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_fwd_8(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
-  switch (fmt) {
-    case SK_FMT_S8: return fwd_launch_one<SK_FMT_S8>(grid, a, st);
-    case SK_FMT_U8: return fwd_launch_one<SK_FMT_U8>(grid, a, st);
-    case SK_FMT_CS8: return fwd_launch_one<SK_FMT_CS8>(grid, a, st);
-    case SK_FMT_CU8: return fwd_launch_one<SK_FMT_CU8>(grid, a, st);
-  }
+#define CASE(F) case F: return fwd_launch_one<F>(grid, a, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr_8(int fmt) {
-  switch (fmt) {
-    case SK_FMT_S8: return fwd_ptr_one<SK_FMT_S8>();
-    case SK_FMT_U8: return fwd_ptr_one<SK_FMT_U8>();
-    case SK_FMT_CS8: return fwd_ptr_one<SK_FMT_CS8>();
-    case SK_FMT_CU8: return fwd_ptr_one<SK_FMT_CU8>();
-  }
+cudaError_t launch_fwd_col_8(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
+#define CASE(F) case F: return fwd_col_launch_one<F>(grid, a, Y, st);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
+  return cudaErrorInvalidValue;
+}
+
+const void* fwd_kernel_ptr_8(int fmt, bool col) {
+#define CASE(F) case F: return fwd_ptr_one<F>(col);
+  switch (fmt) { SK_FOR_FORMATS(CASE) }
+#undef CASE
   return nullptr;
 }
 

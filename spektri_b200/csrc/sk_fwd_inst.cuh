@@ -1,4 +1,4 @@
-// One forward-FFT kernel instance per input format; included by the
+// Forward-FFT kernel instances per input format; included by the
 // sk_fwd_{8,16,32}.cu units, which split the formats by sample width so the
 // instances compile in parallel.
 #pragma once
@@ -14,14 +14,23 @@ cudaError_t fwd_launch_one(int grid, const FwdArgs& a, cudaStream_t st) {
 }
 
 template <int FMT>
+cudaError_t fwd_col_launch_one(int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
+  fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
+  return cudaGetLastError();
+}
+
+template <int FMT>
 cudaError_t fwd_prepare_one() {
-  return cudaFuncSetAttribute(fwd_fft_kernel<TILE_S, TILE_T, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(fwd_fft_kernel<TILE_S, TILE_T, FMT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fwd_col_kernel<TILE_S, TILE_T, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)TILE_SMEM);
 }
 
 template <int FMT>
-const void* fwd_ptr_one() {
-  return (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
+const void* fwd_ptr_one(bool col) {
+  return col ? (const void*)fwd_col_kernel<TILE_S, TILE_T, FMT> : (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
 }
 
 }  // namespace sk

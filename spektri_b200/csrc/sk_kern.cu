@@ -24,13 +24,27 @@ cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr(int fmt) {
+const void* fwd_kernel_ptr(int fmt, bool col) {
   switch (format_bits(fmt)) {
-    case 8: return fwd_kernel_ptr_8(fmt);
-    case 16: return fwd_kernel_ptr_16(fmt);
-    case 32: return fwd_kernel_ptr_32(fmt);
+    case 8: return fwd_kernel_ptr_8(fmt, col);
+    case 16: return fwd_kernel_ptr_16(fmt, col);
+    case 32: return fwd_kernel_ptr_32(fmt, col);
   }
   return nullptr;
+}
+
+cudaError_t launch_fwd_col(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
+  switch (format_bits(fmt)) {
+    case 8: return launch_fwd_col_8(fmt, grid, a, Y, st);
+    case 16: return launch_fwd_col_16(fmt, grid, a, Y, st);
+    case 32: return launch_fwd_col_32(fmt, grid, a, Y, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st) {
+  fwd_row_kernel<TILE_S, TILE_T><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
+  return cudaGetLastError();
 }
 
 const void* welch_kernel_ptr(bool cplx) {
@@ -58,7 +72,8 @@ cudaError_t fcfb_prepare() {
                        (const void*)fcfb_kernel<TILE_S, TILE_T, false, true>,
                        (const void*)fcfb_kernel<TILE_S, TILE_T, false, false>,
                        (const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
-                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>};
+                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>,
+                       (const void*)fwd_row_kernel<TILE_S, TILE_T>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
     if (e != cudaSuccess) return e;

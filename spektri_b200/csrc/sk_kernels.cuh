@@ -148,6 +148,65 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
   }
 }
 
+// Two-pass forward FFT for Nc = R1 * S with R1 >= 16 (Nc up to 2^21).
+// Pass A (columns): a tile holds C = S/R1 consecutive columns j2 of one block;
+// it loads z[j1 S + j2] row by row (coalesced), transposes into R1-point
+// transforms in shared memory, runs them, and stores
+// Y[k1][j2] = W_Nc^{j2 k1} sum_j1 z[j1 S + j2] W_R1^{j1 k1}.
+// Pass B (rows): S-point FFT of row k1 of Y gives Z[k1 + R1 k2], stored at
+// k1 S + k2 — the residue layout the spectrum split reads.
+template <int S, int T, int FMT>
+__global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
+  extern __shared__ float2 sm[];
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int E = S / T, LOGS = ilog2c(S);
+  const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
+  {  // carry, as in fwd_fft_kernel
+    const long long stride = (long long)gridDim.x * T;
+    const long long ncomp = a.overlap * (CPLX ? 2 : 1);
+    const long long base = (a.nnew - a.overlap) * (CPLX ? 2 : 1);
+    for (long long h = (long long)blockIdx.x * T + threadIdx.x; h < ncomp; h += stride)
+      a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
+  }
+  const int LOGR1 = a.log2R1, R1 = 1 << LOGR1, LOGC = LOGS - LOGR1, C = 1 << LOGC;
+  const int b = blockIdx.x >> LOGR1;
+  const int c0 = (blockIdx.x & (R1 - 1)) << LOGC;
+  const long long p0 = (long long)b * a.hop;
+#pragma unroll 4
+  for (int k = 0; k < E; ++k) {
+    const int g = threadIdx.x + k * T;
+    const int j1 = g >> LOGC, col = g & (C - 1);
+    const int jj = (j1 << LOGS) + c0 + col;
+    const float2 z = src.pair(p0 + (CPLX ? jj : 2 * jj));
+    sm[padx((col << LOGR1) + j1)] = make_float2(z.x * a.wscale, z.y * a.wscale);
+  }
+  __syncthreads();
+  tile_fft<-1, S, T>(sm, a.tw_tile, LOGR1);
+  const int shC = a.log2N - a.log2Nc;
+  float2* Yb = Y + ((size_t)b << a.log2Nc);
+#pragma unroll 4
+  for (int k = 0; k < E; ++k) {
+    const int g = threadIdx.x + k * T;
+    const int k1 = g >> LOGC, col = g & (C - 1);
+    float2 v = sm[padx((col << LOGR1) + k1)];
+    if (k1) v = cmul(v, __ldg(&a.tw_big[((c0 + col) * k1) << shC]));
+    Yb[((size_t)k1 << LOGS) + c0 + col] = v;
+  }
+}
+
+template <int S, int T>
+__global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* Y) {
+  extern __shared__ float2 sm[];
+  constexpr int LOGS = ilog2c(S);
+  const int b = blockIdx.x >> a.log2R1, k1 = blockIdx.x & (a.R1 - 1);
+  const size_t off = ((size_t)b << a.log2Nc) + ((size_t)k1 << LOGS);
+  const float2* Yr = Y + off;
+  float2* Zr = a.Z + off;
+  auto load = [&](int, int e) { return __ldg(&Yr[e]); };
+  auto store = [&](int, int o, float2 v) { Zr[o] = v; };
+  tile_pipeline<LOGS, S, T, -1>(sm, 1, a.tw_tile, load, store);
+}
+
 // ----------------------------------------------------------------- Welch split
 
 __device__ __forceinline__ float2 z_at(const SplitArgs& a, const float2* Zb, int m) {

@@ -86,6 +86,7 @@ struct sk_plan {
   float* d_halo[2] = {nullptr, nullptr};
   int halo_cur = 0;
   float2* d_Z = nullptr;
+  float2* d_Y = nullptr;                // column-pass output of the two-pass forward FFT (R1 >= 16)
   float2* d_X = nullptr;
   float* d_acc = nullptr;
   float2* d_w = nullptr;
@@ -125,7 +126,7 @@ namespace {
 int plan_free(sk_plan* pl) {
   if (!pl) return SK_OK;
   DeviceGuard g(pl->p.device);
-  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_X,
+  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->d_tiles, pl->d_list,
                   pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
@@ -239,10 +240,19 @@ WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
   return w;
 }
 
+// The forward FFT kernel(s): one fused kernel for R1 <= 8, else the column
+// pass into d_Y followed by the row pass into d_Z.
+cudaError_t launch_fwd_any(const sk_plan* pl, const FwdArgs& a, cudaStream_t st) {
+  if (pl->R1 <= 8) return launch_fwd(pl->fmt, fwd_grid(pl), a, st);
+  const cudaError_t e = launch_fwd_col(pl->fmt, fwd_grid(pl), a, pl->d_Y, st);
+  if (e != cudaSuccess) return e;
+  return launch_fwd_rows(fwd_grid(pl), a, pl->d_Y, st);
+}
+
 int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
                    std::array<cudaEvent_t, SK_N_STAGES + 1>* ev = nullptr) {
   if (ev) SK_CUDA(cudaEventRecord((*ev)[0], st));
-  SK_CUDA(launch_fwd(pl->fmt, fwd_grid(pl), fwd_args(pl, raw), st));
+  SK_CUDA(launch_fwd_any(pl, fwd_args(pl, raw), st));
   if (ev) SK_CUDA(cudaEventRecord((*ev)[1], st));
   if (welch) SK_CUDA(launch_welch(pl->cplx, welch_args(pl, X, *welch), st));
   else SK_CUDA(launch_split(pl->cplx, pl->B, split_args(pl, X), st));
@@ -289,7 +299,7 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
   const WelchArgs wa = welch_args(pl, pl->d_X, wc);
   if (!pl->graph_exec) {
     SK_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t e1 = launch_fwd(pl->fmt, fwd_grid(pl), fa, pl->stream);
+    const cudaError_t e1 = launch_fwd_any(pl, fa, pl->stream);
     const cudaError_t e2 = launch_welch(pl->cplx, wa, pl->stream);
     const int rc = run_fcfb(pl, pl->d_chans, pl->d_X, true, pl->stream);
     cudaGraph_t g = nullptr;
@@ -303,7 +313,7 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     cudaGraphGetNodes(g, nullptr, &n);
     std::vector<cudaGraphNode_t> nodes(n);
     cudaGraphGetNodes(g, nodes.data(), &n);
-    const void* f_fwd = fwd_kernel_ptr(pl->fmt);
+    const void* f_fwd = fwd_kernel_ptr(pl->fmt, pl->R1 > 8);
     const void* f_welch = welch_kernel_ptr(pl->cplx);
     for (auto nd : nodes) {
       cudaGraphNodeType t;
@@ -323,8 +333,11 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     }
     pl->graph = g;
   } else {
+    // The forward node is fwd_fft_kernel(FwdArgs) or, for R1 > 8, the column
+    // pass fwd_col_kernel(FwdArgs, float2* Y): one pointer per parameter.
     cudaKernelNodeParams p = pl->p_fwd;
-    void* a1[] = {(void*)&fa};
+    float2* y = pl->d_Y;
+    void* a1[] = {(void*)&fa, (void*)&y};
     p.kernelParams = a1;
     p.extra = nullptr;
     SK_CUDA(cudaGraphExecKernelNodeSetParams(pl->graph_exec, pl->node_fwd, &p));
@@ -364,7 +377,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   const int log2N = ilog2_exact(p.fft_size);
   const int log2Nc = log2N - (cplx ? 0 : 1);
   if (log2N < 0 || log2Nc < 2 || log2N < 3) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path needs a power of two >= 8", p.fft_size);
-  const int maxLogNc = TILE_LOGS + 3;   // R1 <= 8
+  const int maxLogNc = TILE_LOGS + 8;   // R1 <= 256
   if (log2Nc > maxLogNc) return fail(SK_ERR_UNSUPPORTED, "FFT size %u exceeds the device limit (complex length %d)", p.fft_size, 1 << maxLogNc);
 
   sk_plan* pl = new sk_plan();
@@ -453,6 +466,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_halo[0], halo_n));
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
   TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
+  if (pl->R1 > 8) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B << pl->log2Nc));
   TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->K));
   TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
   TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
@@ -562,7 +576,7 @@ int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
 int sk_launches_per_call(const sk_plan* pl) {
   if (!pl) return fail(SK_ERR_ARG, "null plan");
   const int fb = pl->ch.empty() ? 0 : (pl->p.mode == SK_MODE_BATCHED ? 1 : (int)pl->ch.size());
-  return 2 + fb;
+  return (pl->R1 > 8 ? 3 : 2) + fb;
 }
 
 int sk_set_weights(sk_plan* pl, int32_t c, const float* w) {
@@ -688,7 +702,7 @@ int sk_spectra_window_device(sk_plan* pl, const void* raw_window, float* X, void
   a.halo_next = nullptr;
   a.overlap = 0;
   a.nnew = pl->total;
-  SK_CUDA(launch_fwd(pl->fmt, fwd_grid(pl), a, st));
+  SK_CUDA(launch_fwd_any(pl, a, st));
   SK_CUDA(launch_split(pl->cplx, pl->B, split_args(pl, (float2*)X), st));
   return SK_OK;
 }

@@ -100,6 +100,13 @@ cudaError_t fwd_prepare_32(int fmt);
 cudaError_t launch_fwd_8(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
 cudaError_t launch_fwd_16(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
 cudaError_t launch_fwd_32(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
+// Two-pass forward FFT (R1 >= 16): column pass from the raw samples into Y,
+// then the row pass from Y into Z.
+cudaError_t launch_fwd_col(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
+cudaError_t launch_fwd_col_8(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
+cudaError_t launch_fwd_col_16(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
+cudaError_t launch_fwd_col_32(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
+cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st);
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st);
 cudaError_t fcfb_prepare();
@@ -107,10 +114,10 @@ cudaError_t fcfb_occupancy(int* ctas_per_sm);
 cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
-const void* fwd_kernel_ptr(int fmt);
-const void* fwd_kernel_ptr_8(int fmt);
-const void* fwd_kernel_ptr_16(int fmt);
-const void* fwd_kernel_ptr_32(int fmt);
+const void* fwd_kernel_ptr(int fmt, bool col);
+const void* fwd_kernel_ptr_8(int fmt, bool col);
+const void* fwd_kernel_ptr_16(int fmt, bool col);
+const void* fwd_kernel_ptr_32(int fmt, bool col);
 const void* welch_kernel_ptr(bool cplx);
 
 }  // namespace sk

@@ -87,12 +87,14 @@ def test_all_formats_small(fmt):
 
 
 @pytest.mark.parametrize("fmt,N", [("s16le", 32768), ("s16le", 65536), ("cs16le", 4096),
-                                   ("cs16le", 16384), ("cs16le", 65536), ("s16le", 8192), ("s16le", 16)])
+                                   ("cs16le", 16384), ("cs16le", 65536), ("s16le", 8192), ("s16le", 16),
+                                   ("cs16le", 1 << 17), ("s16le", 1 << 18), ("cs16le", 1 << 20), ("s16le", 1 << 22)])
 def test_fft_sizes_and_split_paths(fmt, N):
-    """Single-tile FFTs, the residue-split path (Nc = R1 * 8192, R1 = 2..8),
-    and the smallest size."""
+    """Single-tile FFTs, the fused residue split (Nc = R1 * 8192, R1 = 2..8),
+    the two-pass column/row FFT (R1 = 16..256, up to 2^20 complex and 2^22
+    real points) and the smallest size."""
     rng = np.random.default_rng(N)
-    B = 4
+    B = 4 if N <= 1 << 17 else 2
     fs = float(N) * 1000.0
     cplx = fmt.startswith("c")
     ns = [n for n in (4, 64, 512, 2048, 8192) if n <= max(4, N // 2)]
@@ -147,7 +149,7 @@ def test_invalid_parameters_rejected():
     with pytest.raises(SpektriError):
         Plan(1e6, 1000, "s16le", [], ffts_per_buf=2)          # not a power of two
     with pytest.raises(SpektriError):
-        Plan(1e6, 1 << 20, "s16le", [], ffts_per_buf=2)       # beyond the residue-split limit
+        Plan(1e6, 1 << 23, "s16le", [], ffts_per_buf=2)       # beyond 2^21 complex points
     p = Plan(1e6, 1024, "cs16le", [], ffts_per_buf=3)        # odd is fine for complex input
     assert p.n_channels == 0
     p.process(np.zeros(p.raw_bytes, np.uint8))
@@ -171,6 +173,24 @@ def test_c3_shape_plain_equals_batched_and_oracle():
             assert np.array_equal(a, b)
         errs = [rel_rms(a, ref) for a, ref in zip(ob, o)]
         assert max(errs) < TOL, max(errs)
+
+
+def test_c5_shape_complex_channelizer():
+    """The large complex channelizer: cs16 input, forward FFT 2^20 (two-pass),
+    2048 channels of 64..8192, B = 8 — one buffer against the FP64 oracle,
+    spectrum included (64 averages span 8 buffers, so f32 records appear
+    from the 8th call; the first call checks the outputs)."""
+    w = workloads.c5()
+    x = workloads.stream_torch(w, w.samples_per_buffer, "cuda").cpu().numpy()
+    plan = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 8)
+    assert plan.n_channels == 2048
+    o64 = _o64(plan, w.fmt)
+    sp, outs = plan.process(x)
+    sp64, o = o64.process(x)
+    assert [s for s, _ in sp] == [s for s, _ in sp64] == [0]
+    assert rel_rms(sp[0][1], sp64[0][1]) < TOL
+    errs = [rel_rms(a, ref) for a, ref in zip(outs, o)]
+    assert max(errs) < TOL, max(errs)
 
 
 def test_device_path_matches_host_path():
