@@ -229,6 +229,7 @@ def main():
                     averages=w.averages, spectrum_format="f32", mode=mode, device=dev)
 
     plan = make(args.mode)
+    tile_threads, ctas_per_sm, tune_us = plan.autotune()       # cached per device / FFT size / channel mix
     outs = [torch.empty(c["out_samples"], dtype=torch.complex64, device=dev) for c in plan.channels]
     spec = torch.empty(plan.max_spectra * plan.spectrum_bytes, dtype=torch.uint8, device=dev)
     st = torch.cuda.Stream(dev)
@@ -284,6 +285,7 @@ def main():
                    "ffts_per_buf": w.ffts_per_buf, "averages": w.averages, "channels": len(w.channels),
                    "sum_ifft_bins": sum(c["n"] for c in w.channels), "samples_per_step": spb,
                    "parallelism": f"replicas x{ws}",
+                   "tuning": {"tile_threads": tile_threads, "ctas_per_sm": ctas_per_sm, "fcfb_us": round(tune_us, 1)},
                    "l2": f"{nbuf} distinct input buffers cycled ({nbuf * raw_bytes / 1e6:.0f} MB) and "
                          f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2"},
         "hbm_gbs_pipeline": round(value * 1e6 / ws * alg / 1e9, 1),
@@ -304,6 +306,7 @@ def main():
 
     if args.compare_plain and args.mode == "batched":
         pp = make("plain")
+        pp.set_tuning(tile_threads, ctas_per_sm)
         run_steps(pp, args.warmup, 0)
         torch.cuda.synchronize(dev)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -205,6 +205,19 @@ int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W
 int sk_plan_set_timing(sk_plan* plan, int enable);
 int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
 
+/* ------------------------------------------------------------ tuning
+ * The filter bank runs 8192-point tiles of 256 threads (32 elements each) or
+ * 512 threads (16 elements each), with ctas_per_sm persistent CTAs per SM.
+ * sk_plan_autotune times every shape on the plan's own buffers (CUDA events,
+ * 5 launches after 2 warm-ups), applies the fastest and appends it to the
+ * JSON-lines file cache_path (when not NULL) under a key of device, FFT size,
+ * input kind, blocks per buffer and channel mix; a later call with the same
+ * key reads the cache instead of measuring.  Reference counterpart: none (the
+ * reference uses rustfft's planner per size, fcfb.rs:143-150). */
+int sk_plan_autotune(sk_plan* plan, const char* cache_path, double* best_us);
+int sk_plan_set_tuning(sk_plan* plan, int32_t tile_threads, int32_t ctas_per_sm);
+int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_threads, int32_t* ctas_per_sm);
+
 /* ------------------------------------------------------------ allocation-free spectra
  * No counterpart in the reference: an addition for callers that may not
  * allocate device memory — a real-time receive callback that must never

@@ -23,19 +23,30 @@
 namespace sk {
 
 // log2 radices of the stages for a 2^LOGN-point transform.
-template <int LOGN> struct StagePlan;
-template <> struct StagePlan<2> { static constexpr int ns = 1, r0 = 2, r1 = 0, r2 = 0; };
-template <> struct StagePlan<3> { static constexpr int ns = 1, r0 = 3, r1 = 0, r2 = 0; };
-template <> struct StagePlan<4> { static constexpr int ns = 1, r0 = 4, r1 = 0, r2 = 0; };
-template <> struct StagePlan<5> { static constexpr int ns = 2, r0 = 3, r1 = 2, r2 = 0; };
-template <> struct StagePlan<6> { static constexpr int ns = 2, r0 = 3, r1 = 3, r2 = 0; };
-template <> struct StagePlan<7> { static constexpr int ns = 2, r0 = 4, r1 = 3, r2 = 0; };
-template <> struct StagePlan<8> { static constexpr int ns = 2, r0 = 4, r1 = 4, r2 = 0; };
-template <> struct StagePlan<9> { static constexpr int ns = 2, r0 = 4, r1 = 5, r2 = 0; };
-template <> struct StagePlan<10> { static constexpr int ns = 3, r0 = 4, r1 = 3, r2 = 3; };
-template <> struct StagePlan<11> { static constexpr int ns = 3, r0 = 4, r1 = 3, r2 = 4; };
-template <> struct StagePlan<12> { static constexpr int ns = 3, r0 = 4, r1 = 4, r2 = 4; };
-template <> struct StagePlan<13> { static constexpr int ns = 3, r0 = 4, r1 = 4, r2 = 5; };
+// log2 radix of stage p (0 = none) for a 2^logn-point transform with E
+// elements per thread: a stage of radix R needs R <= E, the first stage keeps
+// R <= 16 (its R gathered inputs are live at once).
+__host__ __device__ constexpr int stage_log_radix(int logn, int e, int p) {
+  if (e >= 32) {
+    // 4:[4] 8:[8] 16:[16] 32:[8,4] 64:[8,8] 128:[16,8] 256:[16,16] 512:[16,32]
+    // 1024:[16,8,8] 2048:[16,8,16] 4096:[16,16,16] 8192:[16,16,32]
+    constexpr int t[12][3] = {{2, 0, 0}, {3, 0, 0}, {4, 0, 0}, {3, 2, 0}, {3, 3, 0}, {4, 3, 0},
+                              {4, 4, 0}, {4, 5, 0}, {4, 3, 3}, {4, 3, 4}, {4, 4, 4}, {4, 4, 5}};
+    return p < 3 ? t[logn - 2][p] : 0;
+  }
+  // radix <= 16: ... 512:[8,8,8] 1024:[16,8,8] 2048:[16,16,8] 4096:[16,16,16] 8192:[16,16,16,2]
+  constexpr int u[12][4] = {{2, 0, 0, 0}, {3, 0, 0, 0}, {4, 0, 0, 0}, {3, 2, 0, 0}, {3, 3, 0, 0}, {4, 3, 0, 0},
+                            {4, 4, 0, 0}, {3, 3, 3, 0}, {4, 3, 3, 0}, {4, 4, 3, 0}, {4, 4, 4, 0}, {4, 4, 4, 1}};
+  return u[logn - 2][p];
+}
+
+template <int LOGN, int E>
+struct StagePlan {
+  static constexpr int r0 = stage_log_radix(LOGN, E, 0), r1 = stage_log_radix(LOGN, E, 1),
+                       r2 = stage_log_radix(LOGN, E, 2), r3 = stage_log_radix(LOGN, E, 3);
+  static constexpr int ns = (r0 > 0) + (r1 > 0) + (r2 > 0) + (r3 > 0);
+  static_assert(r0 + r1 + r2 + r3 == LOGN, "stages must cover the transform");
+};
 
 // Stage 1 (span L = 1): butterfly q of transform t reads inputs q + s n/R and
 // writes y[q R + u]; as the only stage (n = R, q = 0) it stores output u.
@@ -128,19 +139,27 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
 template <int LOGN, int S, int T, int DIR, class Load, class Store>
 __device__ __forceinline__ void tile_pipeline(float2* sm, int count, const float2* __restrict__ tw, Load& load,
                                               Store& store) {
-  using P = StagePlan<LOGN>;
+  using P = StagePlan<LOGN, S / T>;
   if constexpr (P::ns == 1) {
     stage_first<LOGN, 1 << P::r0, S, T, DIR, true>(sm, count, load, store);
   } else if constexpr (P::ns == 2) {
     stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, true>(sm, count, tw, store);
-  } else {
+  } else if constexpr (P::ns == 3) {
     stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, true>(sm, count, tw, store);
+  } else {
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, store);
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, true>(sm, count, tw, store);
   }
 }
 

@@ -66,11 +66,23 @@ cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Filter-bank tile shapes: 8192-point tiles with 256 threads (32 elements
+// each, 2 CTAs per SM) or 512 threads (16 elements each, radix <= 16 stages,
+// twice the warps per SM).
+template <int T>
+const void* fcfb_fn(bool cplx, bool persistent) {
+  if (persistent) return cplx ? (const void*)fcfb_kernel<TILE_S, T, true, false> : (const void*)fcfb_kernel<TILE_S, T, true, true>;
+  return cplx ? (const void*)fcfb_kernel<TILE_S, T, false, false> : (const void*)fcfb_kernel<TILE_S, T, false, true>;
+}
+
+const void* fcfb_kernel_ptr(int tile_threads, bool cplx, bool persistent) {
+  return tile_threads == 512 ? fcfb_fn<512>(cplx, persistent) : fcfb_fn<TILE_T>(cplx, persistent);
+}
+
 cudaError_t fcfb_prepare() {
-  const void* fns[] = {(const void*)fcfb_kernel<TILE_S, TILE_T, true, true>,
-                       (const void*)fcfb_kernel<TILE_S, TILE_T, true, false>,
-                       (const void*)fcfb_kernel<TILE_S, TILE_T, false, true>,
-                       (const void*)fcfb_kernel<TILE_S, TILE_T, false, false>,
+  const void* fns[] = {fcfb_fn<TILE_T>(true, true), fcfb_fn<TILE_T>(true, false), fcfb_fn<TILE_T>(false, true),
+                       fcfb_fn<TILE_T>(false, false), fcfb_fn<512>(true, true), fcfb_fn<512>(true, false),
+                       fcfb_fn<512>(false, true), fcfb_fn<512>(false, false),
                        (const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
                        (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>,
                        (const void*)fwd_row_kernel<TILE_S, TILE_T>};
@@ -81,20 +93,18 @@ cudaError_t fcfb_prepare() {
   return cudaSuccess;
 }
 
-cudaError_t fcfb_occupancy(int* per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel<TILE_S, TILE_T, true, true>, TILE_T,
-                                                       TILE_SMEM);
+cudaError_t fcfb_occupancy(int tile_threads, int* per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_threads, false, true),
+                                                       tile_threads, TILE_SMEM);
 }
 
-cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st) {
-  if (persistent) {
-    if (cplx) fcfb_kernel<TILE_S, TILE_T, true, false><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
-    else fcfb_kernel<TILE_S, TILE_T, true, true><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
-  } else {
-    if (cplx) fcfb_kernel<TILE_S, TILE_T, false, false><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
-    else fcfb_kernel<TILE_S, TILE_T, false, true><<<grid, TILE_T, TILE_SMEM, st>>>(a, tile_base);
-  }
-  return cudaGetLastError();
+cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_threads, int grid, const FcfbArgs& a, int tile_base,
+                        cudaStream_t st) {
+  FcfbArgs args = a;
+  int base = tile_base;
+  void* params[] = {(void*)&args, (void*)&base};
+  return cudaLaunchKernel(fcfb_kernel_ptr(tile_threads, cplx, persistent), dim3(grid), dim3(tile_threads), params,
+                          TILE_SMEM, st);
 }
 
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st) {

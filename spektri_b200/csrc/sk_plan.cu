@@ -101,6 +101,9 @@ struct sk_plan {
   int2* d_list = nullptr;
   int* d_cursor = nullptr;
   int persist_grid = 1;
+  int sms = 1;                          // multiprocessors of the device
+  int fcfb_threads = TILE_T;            // filter-bank tile shape (256 or 512 threads per 8192-point tile)
+  int fcfb_ctas_per_sm = 2;             // persistent CTAs per SM
   cudaStream_t stream = nullptr;
   // buffers of the host-pointer path
   uint8_t* d_raw = nullptr;
@@ -281,10 +284,10 @@ int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, c
   if (batched) {
     SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
     const int grid = std::min(pl->persist_grid, pl->n_batched_tiles);
-    SK_CUDA(launch_fcfb(pl->cplx, true, grid, a, 0, st));
+    SK_CUDA(launch_fcfb(pl->cplx, true, pl->fcfb_threads, grid, a, 0, st));
   } else {
     for (size_t c = 0; c < pl->ch.size(); ++c)
-      SK_CUDA(launch_fcfb(pl->cplx, false, pl->plain_count[c], a, pl->plain_start[c], st));
+      SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_threads, pl->plain_count[c], a, pl->plain_start[c], st));
   }
   return SK_OK;
 }
@@ -530,8 +533,10 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   if (!tiles.empty()) CUDA_TRY(cudaMemcpy(pl->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
   int sms = 0, per_sm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
-  CUDA_TRY(fcfb_occupancy(&per_sm));
-  pl->persist_grid = std::max(1, sms * std::max(1, per_sm));
+  CUDA_TRY(fcfb_occupancy(pl->fcfb_threads, &per_sm));
+  pl->sms = std::max(1, sms);
+  pl->fcfb_ctas_per_sm = std::max(1, per_sm);
+  pl->persist_grid = pl->sms * pl->fcfb_ctas_per_sm;
 #undef TRY
 #undef CUDA_TRY
   *out = pl;
@@ -724,7 +729,7 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   }
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
-  SK_CUDA(launch_fcfb(pl->cplx, false, pl->n_batched_tiles, a, 0, st));
+  SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_threads, pl->n_batched_tiles, a, 0, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
@@ -788,6 +793,120 @@ int sk_plan_timing(sk_plan* pl, double* ms, uint64_t* calls) {
   }
   if (calls) *calls = pl->timed_calls;
   pl->timed_calls = 0;
+  return SK_OK;
+}
+
+int sk_plan_set_tuning(sk_plan* pl, int32_t tile_threads, int32_t ctas_per_sm) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (tile_threads != 256 && tile_threads != 512) return fail(SK_ERR_ARG, "tile_threads must be 256 or 512");
+  DeviceGuard g(pl->p.device);
+  int max_per_sm = 0;
+  SK_CUDA(fcfb_occupancy(tile_threads, &max_per_sm));
+  if (ctas_per_sm < 1 || ctas_per_sm > max_per_sm)
+    return fail(SK_ERR_ARG, "ctas_per_sm must be 1..%d for %d-thread tiles", max_per_sm, tile_threads);
+  SK_CUDA(cudaStreamSynchronize(pl->stream));
+  pl->fcfb_threads = tile_threads;
+  pl->fcfb_ctas_per_sm = ctas_per_sm;
+  pl->persist_grid = pl->sms * ctas_per_sm;
+  if (pl->graph_exec) {                 // the captured launch configuration is stale
+    cudaGraphExecDestroy(pl->graph_exec);
+    cudaGraphDestroy(pl->graph);
+    pl->graph_exec = nullptr;
+    pl->graph = nullptr;
+    pl->node_fwd = pl->node_welch = nullptr;
+  }
+  return SK_OK;
+}
+
+int sk_plan_get_tuning(const sk_plan* pl, int32_t* tile_threads, int32_t* ctas_per_sm) {
+  if (check_plan(pl) || !tile_threads || !ctas_per_sm) return fail(SK_ERR_ARG, "null argument");
+  *tile_threads = pl->fcfb_threads;
+  *ctas_per_sm = pl->fcfb_ctas_per_sm;
+  return SK_OK;
+}
+
+int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  if (pl->ch.empty()) return SK_OK;
+  DeviceGuard g(pl->p.device);
+  // Key: device, FFT size and kind, blocks per buffer, and the channel mix
+  // (how many transforms of each IFFT size; FNV-1a of the counts).
+  cudaDeviceProp prop{};
+  SK_CUDA(cudaGetDeviceProperties(&prop, pl->p.device));
+  int counts[14] = {0};
+  for (const auto& c : pl->ch) counts[c.log2n]++;
+  unsigned long long h = 1469598103934665603ull;
+  for (int v : counts) { h ^= (unsigned long long)v; h *= 1099511628211ull; }
+  char key[256];
+  snprintf(key, sizeof key, "%s|N=%lld|complex=%d|B=%d|channels=%zu|mix=%016llx", prop.name, pl->N, (int)pl->cplx,
+           pl->B, pl->ch.size(), h);
+  if (cache_path) {
+    if (FILE* f = fopen(cache_path, "r")) {
+      char line[1024];
+      int tt = 0, cps = 0;
+      double us = 0;
+      bool found = false;
+      while (fgets(line, sizeof line, f)) {
+        const char* k = strstr(line, "\"key\": \"");
+        if (!k || strncmp(k + 8, key, strlen(key)) != 0 || k[8 + strlen(key)] != '"') continue;
+        const char* a = strstr(line, "\"tile_threads\": ");
+        const char* b = strstr(line, "\"ctas_per_sm\": ");
+        const char* c = strstr(line, "\"us\": ");
+        if (a && b && sscanf(a + 16, "%d", &tt) == 1 && sscanf(b + 15, "%d", &cps) == 1) {
+          if (c) sscanf(c + 6, "%lf", &us);
+          found = true;                  // the last matching line wins
+        }
+      }
+      fclose(f);
+      if (found && sk_plan_set_tuning(pl, tt, cps) == SK_OK) {
+        if (best_us) *best_us = us;
+        return SK_OK;
+      }
+    }
+  }
+  // Measure every shape on the plan's own buffers (spectra zeroed, outputs in
+  // the plan's output buffer): 2 warm-up and 5 timed launches each.
+  cudaStream_t st = pl->stream;
+  std::vector<ChanDev> own(pl->h_chans);
+  for (size_t c = 0; c < own.size(); ++c) own[c].out = (float2*)pl->d_out_ptrs[c];
+  SK_CUDA(cudaMemcpyAsync(pl->d_chans_aux, own.data(), sizeof(ChanDev) * own.size(), cudaMemcpyHostToDevice, st));
+  SK_CUDA(cudaMemsetAsync(pl->d_X, 0, sizeof(float2) * (size_t)pl->B * pl->K, st));
+  cudaEvent_t e0, e1;
+  SK_CUDA(cudaEventCreate(&e0));
+  SK_CUDA(cudaEventCreate(&e1));
+  const int shapes[] = {256, 512};
+  int best_t = pl->fcfb_threads, best_c = pl->fcfb_ctas_per_sm;
+  float best = 1e30f;
+  for (int tt : shapes) {
+    int max_per_sm = 0;
+    if (fcfb_occupancy(tt, &max_per_sm) != cudaSuccess) continue;
+    for (int cps = 1; cps <= max_per_sm; ++cps) {
+      FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, pl->d_X);
+      const int grid = std::min(pl->sms * cps, pl->n_batched_tiles);
+      float ms = 0.f;
+      for (int it = 0; it < 7; ++it) {
+        if (it == 2) SK_CUDA(cudaEventRecord(e0, st));
+        SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
+        SK_CUDA(launch_fcfb(pl->cplx, true, tt, grid, a, 0, st));
+      }
+      SK_CUDA(cudaEventRecord(e1, st));
+      SK_CUDA(cudaEventSynchronize(e1));
+      SK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) { best = ms; best_t = tt; best_c = cps; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int rc = sk_plan_set_tuning(pl, best_t, best_c);
+  if (rc) return rc;
+  const double us = best * 1000.0 / 5.0;
+  if (best_us) *best_us = us;
+  if (cache_path) {
+    if (FILE* f = fopen(cache_path, "a")) {
+      fprintf(f, "{\"key\": \"%s\", \"tile_threads\": %d, \"ctas_per_sm\": %d, \"us\": %.3f}\n", key, best_t, best_c, us);
+      fclose(f);
+    }
+  }
   return SK_OK;
 }
 

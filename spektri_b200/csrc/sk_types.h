@@ -110,8 +110,11 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st);
 cudaError_t fcfb_prepare();
-cudaError_t fcfb_occupancy(int* ctas_per_sm);
-cudaError_t launch_fcfb(bool cplx, bool persistent, int grid, const FcfbArgs& a, int tile_base, cudaStream_t st);
+// Filter-bank tile shapes: tile_threads = 256 (32 elements per thread) or 512 (16).
+cudaError_t fcfb_occupancy(int tile_threads, int* ctas_per_sm);
+cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_threads, int grid, const FcfbArgs& a, int tile_base,
+                        cudaStream_t st);
+const void* fcfb_kernel_ptr(int tile_threads, bool cplx, bool persistent);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 const void* fwd_kernel_ptr(int fmt, bool col);

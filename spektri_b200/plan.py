@@ -7,6 +7,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 import weakref
 
 import numpy as np
@@ -196,6 +197,26 @@ class Plan:
         check(lib().sk_process_device(self._h, _ptr(raw), tbl, _ptr(spec) if spec is not None else None,
                                       C.byref(r), stream), "sk_process_device")
         return r
+
+    def autotune(self, cache_path=None):
+        """Pick the filter-bank tile shape and persistent grid by timing (or
+        from the JSON-lines cache).  Returns (tile_threads, ctas_per_sm, us)."""
+        if cache_path is None:
+            cache_path = os.environ.get("SPEKTRI_TUNE_CACHE") or os.path.join(
+                os.path.expanduser("~"), ".cache", "spektri_b200", "tune.jsonl")
+        if cache_path:
+            os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        us = C.c_double()
+        check(lib().sk_plan_autotune(self._h, cache_path.encode() if cache_path else None, C.byref(us)), "sk_plan_autotune")
+        return self.tuning() + (us.value,)
+
+    def set_tuning(self, tile_threads: int, ctas_per_sm: int):
+        check(lib().sk_plan_set_tuning(self._h, int(tile_threads), int(ctas_per_sm)), "sk_plan_set_tuning")
+
+    def tuning(self):
+        t, c = C.c_int32(), C.c_int32()
+        check(lib().sk_plan_get_tuning(self._h, C.byref(t), C.byref(c)))
+        return t.value, c.value
 
     def set_timing(self, enable: bool = True):
         check(lib().sk_plan_set_timing(self._h, int(bool(enable))))

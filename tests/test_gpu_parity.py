@@ -214,6 +214,36 @@ def test_device_path_matches_host_path():
                 assert q1 == q2 and np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("shape", [(256, 1), (512, 1), (512, 2)])
+def test_tile_shapes_against_oracle(shape):
+    """Every filter-bank tile shape the autotuner may pick meets the bar, for
+    every IFFT size 4..8192 (radix plans differ between the shapes)."""
+    N, B = 4096, 4
+    sizes = [4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192]
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * (37 * i + 5)) for i, n in enumerate(sizes)]
+    plan = make_plan(N * 1000.0, N, "s16le", filters, B, 3)
+    plan.set_tuning(*shape)
+    assert plan.tuning() == shape
+    rng = np.random.default_rng(21)
+    from tests.test_oracle import _stream
+    run_compare(plan, "s16le", [_stream("s16le", plan.new_samples, rng) for _ in range(3)])
+
+
+def test_autotune_picks_and_caches(tmp_path):
+    w = workloads.c1()
+    plan = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages)
+    cache = tmp_path / "tune.jsonl"
+    t1 = plan.autotune(str(cache))
+    assert t1[0] in (256, 512) and t1[1] >= 1 and t1[2] > 0
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and '"tile_threads"' in lines[0]
+    plan2 = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages)
+    assert plan2.autotune(str(cache))[:2] == t1[:2]              # read back, not re-measured
+    assert len(cache.read_text().splitlines()) == 1
+    raw = workloads.stream_numpy(w, 0, 2 * w.samples_per_buffer).view(np.uint8)
+    run_compare(plan2, w.fmt, np.split(raw, 2))
+
+
 def test_graph_replay_matches_direct_launches():
     """Batched calls replay a captured CUDA graph (per-call kernel arguments
     patched in); with stage timing on the same plan launches directly.
