@@ -171,6 +171,13 @@ int sk_get_weights(const sk_plan* plan, int32_t channel, float* weights_c64);
 int sk_process(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out, sk_result* result);
 int sk_process_device(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out,
                       sk_result* result, void* stream);
+/* Set the carried samples (main.rs:173): raw holds info.overlap samples in the
+ * plan's input format, the last N/4 samples before the next buffer.  A fresh
+ * plan carries zeros, as the reference's first buffer does (main.rs:165);
+ * setting the carry lets a plan start in the middle of a stream (a time
+ * shard on another GPU, or a restart). */
+int sk_plan_set_carry(sk_plan* plan, const void* raw);
+
 /* Wait for all work the plan enqueued. */
 int sk_synchronize(sk_plan* plan);
 /* Number of device kernels one sk_process_device call launches. */

@@ -85,6 +85,7 @@ PROTOTYPES = [
     ("sk_process", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Result)]),
     ("sk_process_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Result), C.c_void_p]),
     ("sk_synchronize", C.c_int, [C.c_void_p]),
+    ("sk_plan_set_carry", C.c_int, [C.c_void_p, C.c_void_p]),
     ("sk_launches_per_call", C.c_int, [C.c_void_p]),
     ("sk_spectra_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sk_spectra_window_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -680,6 +680,31 @@ int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_o
   return SK_OK;
 }
 
+int sk_plan_set_carry(sk_plan* pl, const void* raw) {
+  if (check_plan(pl) || !raw) return fail(SK_ERR_ARG, "null argument");
+  const int comps = pl->cplx ? 2 : 1;
+  const int bps = format_bytes(pl->fmt) / comps;           // bytes per component
+  std::vector<float> h((size_t)pl->overlap * comps);
+  const uint8_t* p = (const uint8_t*)raw;
+  const int base = pl->fmt & 0x3F;                         // format without its complex bit
+  for (size_t i = 0; i < h.size(); ++i, p += bps) {        // inputformats.rs:65-155
+    float v = 0.f;
+    switch (base) {
+      case SK_FMT_S8: v = (float)(int8_t)p[0]; break;
+      case SK_FMT_S16LE: v = (float)(int16_t)(p[0] | (p[1] << 8)); break;
+      case SK_FMT_S16BE: v = (float)(int16_t)(p[1] | (p[0] << 8)); break;
+      case SK_FMT_F32LE: { uint32_t u = p[0] | (p[1] << 8) | (p[2] << 16) | ((uint32_t)p[3] << 24); std::memcpy(&v, &u, 4); break; }
+      case SK_FMT_F32BE: { uint32_t u = p[3] | (p[2] << 8) | (p[1] << 16) | ((uint32_t)p[0] << 24); std::memcpy(&v, &u, 4); break; }
+      case SK_FMT_U8: v = (float)p[0] - 127.4f; break;
+    }
+    h[i] = v;
+  }
+  DeviceGuard g(pl->p.device);
+  SK_CUDA(cudaStreamSynchronize(pl->stream));
+  SK_CUDA(cudaMemcpy(pl->d_halo[pl->halo_cur], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+  return SK_OK;
+}
+
 int sk_synchronize(sk_plan* pl) {
   if (check_plan(pl)) return SK_ERR_ARG;
   DeviceGuard g(pl->p.device);

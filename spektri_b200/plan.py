@@ -228,6 +228,15 @@ class Plan:
         check(lib().sk_plan_timing(self._h, ms, C.byref(n)), "sk_plan_timing")
         return list(ms), n.value
 
+    def set_carry(self, raw):
+        """Carried samples (the N/4 raw samples before the next buffer), so a
+        plan can start mid-stream: a time shard or a restart."""
+        raw = np.ascontiguousarray(raw).view(np.uint8)
+        need = self.overlap * (self.raw_bytes // self.new_samples)
+        if raw.nbytes != need:
+            raise ValueError(f"carry must be {need} bytes, got {raw.nbytes}")
+        check(lib().sk_plan_set_carry(self._h, raw.ctypes.data), "sk_plan_set_carry")
+
     def synchronize(self):
         check(lib().sk_synchronize(self._h))
 

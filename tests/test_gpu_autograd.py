@@ -36,6 +36,7 @@ def fcfb_ref(X, W, chans, N, real):
 
 
 def rel(a, b):
+    a, b = a.detach(), b.detach()
     return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
 
 

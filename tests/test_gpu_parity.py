@@ -328,3 +328,38 @@ def test_weights_update_and_custom_complex_weights():
     plan.set_weights(2, new)
     o64.channels[2].weights = new.astype(np.complex128)
     run_compare(plan, w.fmt, [r1], o64=o64)
+
+
+@pytest.mark.parametrize("fmt,mode", [("s16le", "batched"), ("cf32le", "plain"), ("u8", "batched")])
+def test_carry_starts_mid_stream(fmt, mode):
+    """A plan primed with the N/4 samples before buffer k reproduces, bit for
+    bit, what a plan that processed the whole stream emits from buffer k on
+    (the time-shard contract): channel records and, at a Welch-window
+    boundary, spectrum records (sequence numbers offset by the records before)."""
+    from spektri_b200 import shard
+    N, B, avg, nbuf = 2048, 4, 8, 8
+    cplx = oracle64.is_complex(fmt)
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * f) for n, f in
+               ((64, -300 if cplx else 300), (256, 512), (16, 100))]
+    plans = [make_plan(N * 1000.0, N, fmt, filters, B, avg, mode=mode) for _ in range(2)]
+    p0 = plans[0]
+    rng = np.random.default_rng(5)
+    from tests.test_oracle import _stream
+    raws = [_stream(fmt, p0.new_samples, rng) for _ in range(nbuf)]
+    stream = np.concatenate([np.frombuffer(r, np.uint8) for r in raws])
+    full = [p0.process(r) for r in raws]
+    bps = p0.raw_bytes // p0.new_samples
+    for k in (shard.window_buffers(B, avg), 3):
+        p1 = make_plan(N * 1000.0, N, fmt, filters, B, avg, mode=mode)
+        p1.set_carry(shard.carry_bytes(stream, k, p0.new_samples, p0.overlap, bps))
+        seq_off = k * B // avg
+        for b in range(k, nbuf):
+            sp, outs = p1.process(raws[b])
+            for a, r in zip(outs, full[b][1]):
+                assert np.array_equal(a, r), (fmt, k, b)
+            if k * B % avg == 0:
+                assert [s + seq_off for s, _ in sp] == [s for s, _ in full[b][0]]
+                for (_, a), (_, r) in zip(sp, full[b][0]):
+                    assert np.array_equal(a, r)
+    with pytest.raises(ValueError):
+        p0.set_carry(np.zeros(3, np.uint8))
