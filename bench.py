@@ -202,7 +202,7 @@ def main():
     ap.add_argument("--compare-plain", action="store_true", help="also time the plain per-channel path")
     ap.add_argument("--ffts-per-buf", type=int, default=0, help="override blocks per buffer (small profiling cases)")
     ap.add_argument("--preroll", type=float, default=1.5, help="seconds of untimed steps while clocks are sampled")
-    ap.add_argument("--tuning", default="", help="THREADS,CTAS_PER_SM: fixed filter-bank tile shape instead of autotuning")
+    ap.add_argument("--tuning", default="", help="SIZE,THREADS,CTAS_PER_SM: fixed filter-bank tile shape instead of autotuning")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_setup()
@@ -232,9 +232,9 @@ def main():
     plan = make(args.mode)
     if args.tuning:
         plan.set_tuning(*[int(v) for v in args.tuning.split(",")])
-        tile_threads, ctas_per_sm, tune_us = plan.tuning() + (None,)
+        tile_size, tile_threads, ctas_per_sm, tune_us = plan.tuning() + (None,)
     else:
-        tile_threads, ctas_per_sm, tune_us = plan.autotune()   # cached per device / FFT size / channel mix
+        tile_size, tile_threads, ctas_per_sm, tune_us = plan.autotune()   # cached per device / FFT size / channel mix
     outs = [torch.empty(c["out_samples"], dtype=torch.complex64, device=dev) for c in plan.channels]
     spec = torch.empty(plan.max_spectra * plan.spectrum_bytes, dtype=torch.uint8, device=dev)
     st = torch.cuda.Stream(dev)
@@ -290,7 +290,7 @@ def main():
                    "ffts_per_buf": w.ffts_per_buf, "averages": w.averages, "channels": len(w.channels),
                    "sum_ifft_bins": sum(c["n"] for c in w.channels), "samples_per_step": spb,
                    "parallelism": f"replicas x{ws}",
-                   "tuning": {"tile_threads": tile_threads, "ctas_per_sm": ctas_per_sm, "fcfb_us": round(tune_us, 1) if tune_us else None,
+                   "tuning": {"tile_size": tile_size, "tile_threads": tile_threads, "ctas_per_sm": ctas_per_sm, "fcfb_us": round(tune_us, 1) if tune_us else None,
                               "source": "fixed" if args.tuning else "autotuned"},
                    "l2": f"{nbuf} distinct input buffers cycled ({nbuf * raw_bytes / 1e6:.0f} MB) and "
                          f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2"},
@@ -312,7 +312,7 @@ def main():
 
     if args.compare_plain and args.mode == "batched":
         pp = make("plain")
-        pp.set_tuning(tile_threads, ctas_per_sm)
+        pp.set_tuning(tile_size, tile_threads, ctas_per_sm)
         run_steps(pp, args.warmup, 0)
         torch.cuda.synchronize(dev)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

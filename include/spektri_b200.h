@@ -213,8 +213,10 @@ int sk_plan_set_timing(sk_plan* plan, int enable);
 int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
 
 /* ------------------------------------------------------------ tuning
- * The filter bank runs 8192-point tiles of 256 threads (32 elements each) or
- * 512 threads (16 elements each), with ctas_per_sm persistent CTAs per SM.
+ * The filter bank runs tiles of tile_size points and tile_threads threads:
+ * 8192 x 256 (32 elements per thread), 8192 x 512 (16) or 4096 x 256 (16; an
+ * 8192-point IFFT then runs as two independent 4096-point halves, one per
+ * output parity), with ctas_per_sm persistent CTAs per SM.
  * sk_plan_autotune times every shape on the plan's own buffers (CUDA events,
  * 5 launches after 2 warm-ups), applies the fastest and appends it to the
  * JSON-lines file cache_path (when not NULL) under a key of device, FFT size,
@@ -222,8 +224,8 @@ int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
  * key reads the cache instead of measuring.  Reference counterpart: none (the
  * reference uses rustfft's planner per size, fcfb.rs:143-150). */
 int sk_plan_autotune(sk_plan* plan, const char* cache_path, double* best_us);
-int sk_plan_set_tuning(sk_plan* plan, int32_t tile_threads, int32_t ctas_per_sm);
-int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_threads, int32_t* ctas_per_sm);
+int sk_plan_set_tuning(sk_plan* plan, int32_t tile_size, int32_t tile_threads, int32_t ctas_per_sm);
+int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_size, int32_t* tile_threads, int32_t* ctas_per_sm);
 
 /* ------------------------------------------------------------ allocation-free spectra
  * No counterpart in the reference: an addition for callers that may not

@@ -93,8 +93,8 @@ PROTOTYPES = [
     ("sk_fcfb_backward_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p]),
     ("sk_plan_autotune", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)]),
-    ("sk_plan_set_tuning", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
-    ("sk_plan_get_tuning", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("sk_plan_set_tuning", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    ("sk_plan_get_tuning", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("sk_plan_set_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("sk_plan_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("sk_spectra_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),

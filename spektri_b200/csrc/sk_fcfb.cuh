@@ -10,9 +10,10 @@
 //   middle stage: shared -> twiddle -> DFT_R -> shared (in place)
 //   last stage  : shared -> twiddle -> DFT_R -> store(t, o, v) for output o
 // Shared memory is touched twice per element per middle/last stage; the first
-// and last stages keep one butterfly live at a time (their other side is
-// global memory, so there is no in-place hazard) and stay rolled over
-// butterflies to keep each size's code small.
+// and last stages have global memory on their other side, so there is no
+// in-place hazard: the last stage stays rolled over butterflies (one live at a
+// time), the first is unrolled where the caller asks (UNROLL: all gathers of
+// a thread in flight at once) and rolled otherwise.
 //
 // Users: fcfb_tile (filter bank: gather x weights, inverse FFT, keep
 // [n/8, 7(n/8)), fcfb.rs:154-188) and the forward FFT kernel.
@@ -48,13 +49,48 @@ struct StagePlan {
   static_assert(r0 + r1 + r2 + r3 == LOGN, "stages must cover the transform");
 };
 
+// v[s] *= w^s for s = 1..R-1 with w = W_8192^(j << SH) (conjugated for DIR > 0).
+// Only w^1, w^4 and w^16 come from the table; the other powers are products
+// of at most three of them (w^(16a + 4b + c) = w^16a * w^4b * w^c), which
+// keeps each twiddle within a few ulps while cutting the scattered table
+// reads of a radix-R stage from R-1 to at most 3.
+template <int R, int SH, int DIR>
+__device__ __forceinline__ void twiddle_powers(float2* v, const float2* __restrict__ tw, int j) {
+  auto ld = [&](int s) {
+    float2 w = __ldg(&tw[(j * s) << SH]);                // forward W_S; inverse uses its conjugate
+    if (DIR > 0) w.y = -w.y;
+    return w;
+  };
+  float2 lo[4], mid[4];                                  // w^c (c < 4), w^4b (b < 4)
+  lo[1] = ld(1);
+  if constexpr (R > 2) lo[2] = cmul(lo[1], lo[1]);
+  if constexpr (R > 3) lo[3] = cmul(lo[2], lo[1]);
+  if constexpr (R > 4) mid[1] = ld(4);
+  if constexpr (R > 8) mid[2] = cmul(mid[1], mid[1]);
+  if constexpr (R > 12) mid[3] = cmul(mid[2], mid[1]);
+  float2 hi = make_float2(1.f, 0.f);
+  if constexpr (R > 16) hi = ld(16);
+#pragma unroll
+  for (int s = 1; s < R; ++s) {
+    const int a = s >> 4, b = (s >> 2) & 3, c = s & 3;
+    float2 w;
+    if (b == 0 && a == 0) w = lo[c];
+    else {
+      w = b ? mid[b] : hi;
+      if (a && b) w = cmul(hi, w);
+      if (c) w = cmul(w, lo[c]);
+    }
+    v[s] = cmul(v[s], w);
+  }
+}
+
 // Stage 1 (span L = 1): butterfly q of transform t reads inputs q + s n/R and
 // writes y[q R + u]; as the only stage (n = R, q = 0) it stores output u.
-template <int LOGN, int R, int S, int T, int DIR, bool LAST, class Load, class Store>
+template <int LOGN, int R, int S, int T, int DIR, bool LAST, bool UNROLL, class Load, class Store>
 __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, Store& store) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   static_assert(NB >= 1, "radix too large for the tile");
-#pragma unroll 1
+#pragma unroll (UNROLL ? NB : 1)
   for (int bb = 0; bb < NB; ++bb) {
     const int beta = threadIdx.x + bb * T;
     const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
@@ -83,16 +119,9 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
 template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store>
 __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
-  constexpr int LOGS = ilog2c(S), SH = LOGS - LOGL - LOGR;
+  constexpr int SH = TILE_LOGS - LOGL - LOGR;            // tw is the 2^13-point table
   static_assert(NB >= 1 && SH >= 0, "bad stage");
-  auto twiddle = [&](float2* v, int j) {
-#pragma unroll
-    for (int s = 1; s < R; ++s) {
-      float2 w = __ldg(&tw[(j * s) << SH]);              // forward W_S; inverse uses its conjugate
-      if (DIR > 0) w.y = -w.y;
-      v[s] = cmul(v[s], w);
-    }
-  };
+  auto twiddle = [&](float2* v, int j) { twiddle_powers<R, SH, DIR>(v, tw, j); };
   if constexpr (LAST) {
 #pragma unroll 1
     for (int bb = 0; bb < NB; ++bb) {
@@ -136,24 +165,24 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
 
 // The whole transform of every tile entry.  The caller syncs before (shared
 // memory free) and after (if it reuses shared memory).
-template <int LOGN, int S, int T, int DIR, class Load, class Store>
+template <int LOGN, int S, int T, int DIR, bool UNROLL, class Load, class Store>
 __device__ __forceinline__ void tile_pipeline(float2* sm, int count, const float2* __restrict__ tw, Load& load,
                                               Store& store) {
   using P = StagePlan<LOGN, S / T>;
   if constexpr (P::ns == 1) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, true>(sm, count, load, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, true, UNROLL>(sm, count, load, store);
   } else if constexpr (P::ns == 2) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, true>(sm, count, tw, store);
   } else if constexpr (P::ns == 3) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, true>(sm, count, tw, store);
   } else {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false>(sm, count, load, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
     __syncthreads();
@@ -174,17 +203,20 @@ struct TileMeta {
 
 struct FcfbTileConst {
   int N, K;
-  const float2* tw;    // W_S^k
+  const float2* tw;    // W_8192^k, k < 8192
 };
 
 // get_bin for the gather: bin m (already reduced modulo N) of one block.
 template <bool REAL>
 __device__ __forceinline__ float2 spectrum_bin(const float2* __restrict__ X, int m, int N, int K) {
-  if (REAL && m >= K) {
-    const float2 v = __ldg(&X[N - m]);
-    return make_float2(v.x, -v.y);
+  if constexpr (!REAL) {
+    return __ldg(&X[m]);
+  } else {                                                  // one load, mirror by selects
+    const bool mirror = m >= K;
+    float2 v = __ldg(&X[mirror ? N - m : m]);
+    v.y = mirror ? -v.y : v.y;
+    return v;
   }
-  return __ldg(&X[m]);
 }
 
 template <int LOGN, int S, int T, bool REAL>
@@ -201,12 +233,46 @@ __device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int 
       if ((unsigned)o < (unsigned)keep) meta[t].out[o] = v;
     }
   };
-  tile_pipeline<LOGN, S, T, +1>(sm, count, c.tw, load, store);
+  tile_pipeline<LOGN, S, T, +1, true>(sm, count, c.tw, load, store);
+}
+
+// One half of an n = 2S transform in an S-point tile (count = 1, meta.pad =
+// h).  With buf the shifted, weighted input (buf[i] = W[j] bin(first + j),
+// j = (i + n/2) mod n), the inverse DFT splits by output parity:
+//   y[2k]     = IDFT_{n/2}( buf[i] + buf[i + n/2] )[k]
+//   y[2k + 1] = IDFT_{n/2}( (buf[i] - buf[i + n/2]) e^{+2 pi i i/n} )[k]
+// so the two halves are independent S-point transforms; each gathers both
+// buf[i] (j = i + n/2) and buf[i + n/2] (j = i) and keeps its parity of
+// [n/8, 7(n/8)).
+template <int S, int T, bool REAL>
+__device__ __forceinline__ void fcfb_tile_half(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
+  constexpr int LOGS = ilog2c(S), n = 2 * S, lo = n >> 3, keep = 6 * lo;
+  static_assert(n == (1 << TILE_LOGS), "the split twiddle is the 2^13-point table");
+  const TileMeta& m = meta[0];
+  const int h = m.pad;
+  auto load = [&](int, int i) {
+    const int N1 = c.N - 1;
+    const float2 a = cmul(__ldg(&m.w[i + S]), spectrum_bin<REAL>(m.X, (m.first + i + S) & N1, c.N, c.K));
+    const float2 b = cmul(__ldg(&m.w[i]), spectrum_bin<REAL>(m.X, (m.first + i) & N1, c.N, c.K));
+    if (h == 0) return cadd(a, b);
+    const float2 w = __ldg(&c.tw[i]);                       // e^{-2 pi i i/n}; conjugated below
+    return cmul(csub(a, b), make_float2(w.x, -w.y));
+  };
+  auto store = [&](int, int o, float2 v) {
+    const int k = 2 * o + h - lo;
+    if ((unsigned)k < (unsigned)keep) m.out[k] = v;
+  };
+  tile_pipeline<LOGS, S, T, +1, true>(sm, 1, c.tw, load, store);
 }
 
 template <int S, int T, bool REAL>
 __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const TileMeta* meta, int count,
                                                    const FcfbTileConst& c) {
+  constexpr int LOGS = ilog2c(S);
+  if (log2n > LOGS) {
+    if constexpr (LOGS < TILE_LOGS) fcfb_tile_half<S, T, REAL>(sm, meta, c);
+    return;
+  }
   switch (log2n) {
     case 2: fcfb_tile<2, S, T, REAL>(sm, meta, count, c); break;
     case 3: fcfb_tile<3, S, T, REAL>(sm, meta, count, c); break;
@@ -218,8 +284,8 @@ __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const 
     case 9: fcfb_tile<9, S, T, REAL>(sm, meta, count, c); break;
     case 10: fcfb_tile<10, S, T, REAL>(sm, meta, count, c); break;
     case 11: fcfb_tile<11, S, T, REAL>(sm, meta, count, c); break;
-    case 12: fcfb_tile<12, S, T, REAL>(sm, meta, count, c); break;
-    case 13: fcfb_tile<13, S, T, REAL>(sm, meta, count, c); break;
+    case 12: if constexpr (LOGS >= 12) fcfb_tile<12, S, T, REAL>(sm, meta, count, c); break;
+    case 13: if constexpr (LOGS >= 13) fcfb_tile<13, S, T, REAL>(sm, meta, count, c); break;
   }
 }
 

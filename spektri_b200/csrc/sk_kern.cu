@@ -66,24 +66,39 @@ cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// Filter-bank tile shapes: 8192-point tiles with 256 threads (32 elements
-// each, 2 CTAs per SM) or 512 threads (16 elements each, radix <= 16 stages,
-// twice the warps per SM).
-template <int T>
+// Filter-bank tile shapes (tile size x threads, minimum CTAs per SM):
+// 8192 x 256 (32 elements per thread, 2 CTAs/SM), 8192 x 512 (16 elements,
+// radix <= 16 stages, 2 CTAs/SM), 4096 x 256 (16 elements, n = 8192 as two
+// independent halves, FCFB_MINB_4096 CTAs/SM).
+#ifndef FCFB_MINB_4096
+#define FCFB_MINB_4096 4
+#endif
+template <int S, int T, int MINB>
 const void* fcfb_fn(bool cplx, bool persistent) {
-  if (persistent) return cplx ? (const void*)fcfb_kernel<TILE_S, T, true, false> : (const void*)fcfb_kernel<TILE_S, T, true, true>;
-  return cplx ? (const void*)fcfb_kernel<TILE_S, T, false, false> : (const void*)fcfb_kernel<TILE_S, T, false, true>;
+  if (persistent)
+    return cplx ? (const void*)fcfb_kernel<S, T, MINB, true, false> : (const void*)fcfb_kernel<S, T, MINB, true, true>;
+  return cplx ? (const void*)fcfb_kernel<S, T, MINB, false, false> : (const void*)fcfb_kernel<S, T, MINB, false, true>;
 }
 
-const void* fcfb_kernel_ptr(int tile_threads, bool cplx, bool persistent) {
-  return tile_threads == 512 ? fcfb_fn<512>(cplx, persistent) : fcfb_fn<TILE_T>(cplx, persistent);
+bool fcfb_shape_ok(int tile_size, int tile_threads) {
+  return (tile_size == 8192 && (tile_threads == 256 || tile_threads == 512)) ||
+         (tile_size == 4096 && tile_threads == 256);
+}
+
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent) {
+  if (tile_size == 4096) return fcfb_fn<4096, 256, FCFB_MINB_4096>(cplx, persistent);
+  return tile_threads == 512 ? fcfb_fn<TILE_S, 512, 2>(cplx, persistent) : fcfb_fn<TILE_S, TILE_T, 2>(cplx, persistent);
 }
 
 cudaError_t fcfb_prepare() {
-  const void* fns[] = {fcfb_fn<TILE_T>(true, true), fcfb_fn<TILE_T>(true, false), fcfb_fn<TILE_T>(false, true),
-                       fcfb_fn<TILE_T>(false, false), fcfb_fn<512>(true, true), fcfb_fn<512>(true, false),
-                       fcfb_fn<512>(false, true), fcfb_fn<512>(false, false),
-                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
+  const int shapes[][2] = {{8192, 256}, {8192, 512}, {4096, 256}};
+  for (const auto& sh : shapes)
+    for (int k = 0; k < 4; ++k) {
+      const cudaError_t e = cudaFuncSetAttribute(fcfb_kernel_ptr(sh[0], sh[1], k & 1, k & 2),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcfb_smem(sh[0]));
+      if (e != cudaSuccess) return e;
+    }
+  const void* fns[] = {(const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
                        (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>,
                        (const void*)fwd_row_kernel<TILE_S, TILE_T>};
   for (const void* f : fns) {
@@ -93,18 +108,18 @@ cudaError_t fcfb_prepare() {
   return cudaSuccess;
 }
 
-cudaError_t fcfb_occupancy(int tile_threads, int* per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_threads, false, true),
-                                                       tile_threads, TILE_SMEM);
+cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_size, tile_threads, false, true),
+                                                       tile_threads, fcfb_smem(tile_size));
 }
 
-cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_threads, int grid, const FcfbArgs& a, int tile_base,
-                        cudaStream_t st) {
+cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
+                        int tile_base, cudaStream_t st) {
   FcfbArgs args = a;
   int base = tile_base;
   void* params[] = {(void*)&args, (void*)&base};
-  return cudaLaunchKernel(fcfb_kernel_ptr(tile_threads, cplx, persistent), dim3(grid), dim3(tile_threads), params,
-                          TILE_SMEM, st);
+  return cudaLaunchKernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent), dim3(grid), dim3(tile_threads),
+                          params, fcfb_smem(tile_size), st);
 }
 
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st) {

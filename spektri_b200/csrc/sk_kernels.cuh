@@ -77,7 +77,7 @@ __device__ __forceinline__ void fwd_tile_blocks(float2* sm, const FwdArgs& a, co
     return make_float2(z.x * a.wscale, z.y * a.wscale);
   };
   auto store = [&](int t, int o, float2 v) { a.Z[((size_t)(b0 + t) << LOGN) + o] = v; };
-  tile_pipeline<LOGN, S, T, -1>(sm, count, a.tw_tile, load, store);
+  tile_pipeline<LOGN, S, T, -1, false>(sm, count, a.tw_tile, load, store);
 }
 
 // One residue class k1 of one block (Nc = R1 S): element j2 of the tile is
@@ -108,7 +108,7 @@ __device__ __forceinline__ void fwd_tile_split(float2* sm, const FwdArgs& a, con
     return acc;
   };
   auto store = [&](int, int o, float2 v) { Zb[o] = v; };
-  tile_pipeline<LOGS, S, T, -1>(sm, 1, a.tw_tile, load, store);
+  tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
 }
 
 template <int S, int T, int FMT>
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* 
   float2* Zr = a.Z + off;
   auto load = [&](int, int e) { return __ldg(&Yr[e]); };
   auto store = [&](int, int o, float2 v) { Zr[o] = v; };
-  tile_pipeline<LOGS, S, T, -1>(sm, 1, a.tw_tile, load, store);
+  tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
 }
 
 // ----------------------------------------------------------------- Welch split
@@ -327,20 +327,26 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
 }
 
 // ----------------------------------------------------------------- filter bank
-template <int S, int T, bool PERSIST, bool REAL>
-__global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
+template <int S, int T, int MINB, bool PERSIST, bool REAL>
+__global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base) {
   extern __shared__ float2 sm[];
   __shared__ TileMeta s_meta[MAX_TILE_TRANSFORMS];
-  __shared__ int s_tile;
+  __shared__ int s_tile[2];
   static_assert(MAX_TILE_TRANSFORMS <= T, "one thread stages one transform's metadata");
+  // Persistent: thread 0 claims tile it+1 while tile it is being transformed
+  // (the claim's latency hides behind the FFT), publishing it in s_tile[(it+1)&1]
+  // just before the barrier that starts iteration it+1.
+  if constexpr (PERSIST) {
+    if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.cursor, 1);
+  }
   for (int it = 0;; ++it) {
     const FcfbTileConst c{1 << a.log2N, a.K, a.tw};
-    int tile;
+    int tile, next = 0;
     if constexpr (PERSIST) {
-      if (threadIdx.x == 0) s_tile = atomicAdd(a.cursor, 1);
       __syncthreads();               // also orders the previous tile's reads before this tile's writes
-      tile = s_tile;
+      tile = s_tile[it & 1];
       if (tile >= a.ntiles) return;
+      if (threadIdx.x == 0) next = atomicAdd(a.cursor, 1);
     } else {
       if (it) return;
       tile = tile_base + blockIdx.x;
@@ -350,16 +356,21 @@ __global__ void __launch_bounds__(T, 2) fcfb_kernel(FcfbArgs a, int tile_base) {
       const int2 cb = __ldg(&a.list[td.list_off + threadIdx.x]);
       const ChanDev& ch = a.chans[cb.x];
       const int keep = 6 * ((1 << td.log2n) >> 3);
+      const bool half = td.log2n > ilog2c(S);                // entry (channel, 2 block + half)
+      const int b = half ? cb.y >> 1 : cb.y;
       TileMeta m;
-      m.X = a.X + (size_t)cb.y * a.K;
+      m.X = a.X + (size_t)b * a.K;
       m.w = ch.w;
-      m.out = ch.out + (size_t)cb.y * keep;
+      m.out = ch.out + (size_t)b * keep;
       m.first = (int)(ch.first & (long long)(c.N - 1));
-      m.pad = 0;
+      m.pad = half ? (cb.y & 1) : 0;
       s_meta[threadIdx.x] = m;
     }
     __syncthreads();
     fcfb_tile_dispatch<S, T, REAL>(td.log2n, sm, s_meta, td.count, c);
+    if constexpr (PERSIST) {
+      if (threadIdx.x == 0) s_tile[(it + 1) & 1] = next;
+    }
   }
 }
 

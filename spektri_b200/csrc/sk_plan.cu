@@ -95,14 +95,19 @@ struct sk_plan {
   std::vector<ChanDev> h_chans_uploaded;
   ChanDev* d_chans_aux = nullptr;
   BwdChan* d_bwd = nullptr;
-  TileDesc* d_tiles = nullptr;
-  int n_batched_tiles = 0;
-  std::vector<int> plain_start, plain_count;
-  int2* d_list = nullptr;
+  struct TileSet {                      // filter-bank work list for one tile size
+    int size = 0;
+    TileDesc* d_tiles = nullptr;        // batched tiles first, then each channel's own (plain mode)
+    int2* d_list = nullptr;             // (channel, block), or (channel, 2 block + half) for n = 2 size
+    int n_batched = 0;
+    std::vector<int> plain_start, plain_count;
+  };
+  TileSet ts[2];                        // 8192-point tiles (also the adjoint's) and 4096-point tiles
   int* d_cursor = nullptr;
   int persist_grid = 1;
   int sms = 1;                          // multiprocessors of the device
-  int fcfb_threads = TILE_T;            // filter-bank tile shape (256 or 512 threads per 8192-point tile)
+  int fcfb_size = TILE_S;               // filter-bank tile shape: points per tile,
+  int fcfb_threads = TILE_T;            // threads per tile,
   int fcfb_ctas_per_sm = 2;             // persistent CTAs per SM
   cudaStream_t stream = nullptr;
   // buffers of the host-pointer path
@@ -130,8 +135,8 @@ int plan_free(sk_plan* pl) {
   if (!pl) return SK_OK;
   DeviceGuard g(pl->p.device);
   void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
-                  pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->d_tiles, pl->d_list,
-                  pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
+                  pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->ts[0].d_tiles, pl->ts[0].d_list,
+                  pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
   if (pl->graph) cudaGraphDestroy(pl->graph);
   for (void* q : ptrs) if (q) cudaFree(q);
@@ -264,12 +269,15 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* 
   return SK_OK;
 }
 
+const sk_plan::TileSet& cur_tiles(const sk_plan* pl) { return pl->ts[pl->fcfb_size == TILE_S ? 0 : 1]; }
+
 FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
+  const sk_plan::TileSet& t = cur_tiles(pl);
   FcfbArgs a{};
-  a.tiles = pl->d_tiles;
-  a.ntiles = pl->n_batched_tiles;
+  a.tiles = t.d_tiles;
+  a.ntiles = t.n_batched;
   a.cursor = pl->d_cursor;
-  a.list = pl->d_list;
+  a.list = t.d_list;
   a.chans = chans;
   a.X = X;
   a.K = pl->K;
@@ -281,13 +289,14 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
 int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, chans, X);
+  const sk_plan::TileSet& t = cur_tiles(pl);
   if (batched) {
     SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
-    const int grid = std::min(pl->persist_grid, pl->n_batched_tiles);
-    SK_CUDA(launch_fcfb(pl->cplx, true, pl->fcfb_threads, grid, a, 0, st));
+    const int grid = std::min(pl->persist_grid, t.n_batched);
+    SK_CUDA(launch_fcfb(pl->cplx, true, pl->fcfb_size, pl->fcfb_threads, grid, a, 0, st));
   } else {
     for (size_t c = 0; c < pl->ch.size(); ++c)
-      SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_threads, pl->plain_count[c], a, pl->plain_start[c], st));
+      SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a, t.plain_start[c], st));
   }
   return SK_OK;
 }
@@ -504,36 +513,53 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     CUDA_TRY(cudaMemcpy(pl->d_chans, pl->h_chans.data(), sizeof(ChanDev) * pl->h_chans.size(), cudaMemcpyHostToDevice));
   pl->h_chans_uploaded = pl->h_chans;
 
-  // Work lists.  Batched: channels grouped by IFFT size, largest first, each
-  // size's (channel, block) transforms packed S/n to a tile.  Plain: each
-  // channel's own tiles.
-  std::vector<int2> list;
-  std::vector<TileDesc> tiles;
-  for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
-    const int per = std::min(S >> l2, MAX_TILE_TRANSFORMS);
-    const int base = (int)list.size();
-    for (size_t c = 0; c < pl->ch.size(); ++c)
-      if (pl->ch[c].log2n == l2)
-        for (int b = 0; b < pl->B; ++b) list.push_back(make_int2((int)c, b));
-    const int cnt = (int)list.size() - base;
-    for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
+  // Work lists, one per tile size.  Batched: channels grouped by IFFT size,
+  // largest first, each size's (channel, block) transforms packed size/n to a
+  // tile (an n = 2 size transform takes two tiles, one per output parity).
+  // Plain: each channel's own tiles.
+  for (int k = 0; k < 2; ++k) {
+    sk_plan::TileSet& t = pl->ts[k];
+    t.size = k == 0 ? TILE_S : TILE_S / 2;
+    const int logt = k == 0 ? TILE_LOGS : TILE_LOGS - 1;
+    std::vector<int2> list;
+    std::vector<TileDesc> tiles;
+    auto add = [&](int c, int l2) {     // one channel's transforms onto the list
+      for (int b = 0; b < pl->B; ++b)
+        if (l2 > logt) {
+          list.push_back(make_int2(c, 2 * b));
+          list.push_back(make_int2(c, 2 * b + 1));
+        } else {
+          list.push_back(make_int2(c, b));
+        }
+    };
+    auto per_tile = [&](int l2) { return l2 > logt ? 1 : std::min(t.size >> l2, MAX_TILE_TRANSFORMS); };
+    for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
+      const int base = (int)list.size();
+      for (size_t c = 0; c < pl->ch.size(); ++c)
+        if (pl->ch[c].log2n == l2) add((int)c, l2);
+      const int cnt = (int)list.size() - base, per = per_tile(l2);
+      for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
+    }
+    t.n_batched = (int)tiles.size();
+    for (size_t c = 0; c < pl->ch.size(); ++c) {
+      const int l2 = pl->ch[c].log2n, per = per_tile(l2);
+      const int base = (int)list.size();
+      add((int)c, l2);
+      const int cnt = (int)list.size() - base;
+      t.plain_start.push_back((int)tiles.size());
+      for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
+      t.plain_count.push_back((int)tiles.size() - t.plain_start.back());
+    }
+    TRY(dev_alloc(&t.d_list, list.size()));
+    TRY(dev_alloc(&t.d_tiles, tiles.size()));
+    if (!list.empty())
+      CUDA_TRY(cudaMemcpy(t.d_list, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice));
+    if (!tiles.empty())
+      CUDA_TRY(cudaMemcpy(t.d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
   }
-  pl->n_batched_tiles = (int)tiles.size();
-  for (size_t c = 0; c < pl->ch.size(); ++c) {
-    const int l2 = pl->ch[c].log2n, per = std::min(S >> l2, MAX_TILE_TRANSFORMS);
-    const int base = (int)list.size();
-    for (int b = 0; b < pl->B; ++b) list.push_back(make_int2((int)c, b));
-    pl->plain_start.push_back((int)tiles.size());
-    for (int o = 0; o < pl->B; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, pl->B - o), 0});
-    pl->plain_count.push_back((int)tiles.size() - pl->plain_start.back());
-  }
-  TRY(dev_alloc(&pl->d_list, list.size()));
-  TRY(dev_alloc(&pl->d_tiles, tiles.size()));
-  if (!list.empty()) CUDA_TRY(cudaMemcpy(pl->d_list, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice));
-  if (!tiles.empty()) CUDA_TRY(cudaMemcpy(pl->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
   int sms = 0, per_sm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
-  CUDA_TRY(fcfb_occupancy(pl->fcfb_threads, &per_sm));
+  CUDA_TRY(fcfb_occupancy(pl->fcfb_size, pl->fcfb_threads, &per_sm));
   pl->sms = std::max(1, sms);
   pl->fcfb_ctas_per_sm = std::max(1, per_sm);
   pl->persist_grid = pl->sms * pl->fcfb_ctas_per_sm;
@@ -754,7 +780,7 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   }
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
-  SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_threads, pl->n_batched_tiles, a, 0, st));
+  SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_size, pl->fcfb_threads, cur_tiles(pl).n_batched, a, 0, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
@@ -779,15 +805,15 @@ int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, 
   SK_CUDA(cudaMemcpyAsync(pl->d_bwd, bc.data(), sizeof(BwdChan) * bc.size(), cudaMemcpyHostToDevice, st));
   SK_CUDA(cudaStreamSynchronize(st));
   BwdArgs a{};
-  a.tiles = pl->d_tiles;
-  a.list = pl->d_list;
+  a.tiles = pl->ts[0].d_tiles;          // the adjoint runs on 8192-point tiles
+  a.list = pl->ts[0].d_list;
   a.chans = pl->d_bwd;
   a.X = (const float2*)X;
   a.dX = (float2*)dX;
   a.K = pl->K;
   a.log2N = pl->log2N;
   a.tw = pl->d_tw_tile;
-  SK_CUDA(launch_fcfb_backward(pl->cplx, pl->n_batched_tiles, a, st));
+  SK_CUDA(launch_fcfb_backward(pl->cplx, pl->ts[0].n_batched, a, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
@@ -821,15 +847,17 @@ int sk_plan_timing(sk_plan* pl, double* ms, uint64_t* calls) {
   return SK_OK;
 }
 
-int sk_plan_set_tuning(sk_plan* pl, int32_t tile_threads, int32_t ctas_per_sm) {
+int sk_plan_set_tuning(sk_plan* pl, int32_t tile_size, int32_t tile_threads, int32_t ctas_per_sm) {
   if (check_plan(pl)) return SK_ERR_ARG;
-  if (tile_threads != 256 && tile_threads != 512) return fail(SK_ERR_ARG, "tile_threads must be 256 or 512");
+  if (!fcfb_shape_ok(tile_size, tile_threads))
+    return fail(SK_ERR_ARG, "tile shape %d x %d: use 8192 x 256, 8192 x 512 or 4096 x 256", tile_size, tile_threads);
   DeviceGuard g(pl->p.device);
   int max_per_sm = 0;
-  SK_CUDA(fcfb_occupancy(tile_threads, &max_per_sm));
+  SK_CUDA(fcfb_occupancy(tile_size, tile_threads, &max_per_sm));
   if (ctas_per_sm < 1 || ctas_per_sm > max_per_sm)
-    return fail(SK_ERR_ARG, "ctas_per_sm must be 1..%d for %d-thread tiles", max_per_sm, tile_threads);
+    return fail(SK_ERR_ARG, "ctas_per_sm must be 1..%d for %d x %d tiles", max_per_sm, tile_size, tile_threads);
   SK_CUDA(cudaStreamSynchronize(pl->stream));
+  pl->fcfb_size = tile_size;
   pl->fcfb_threads = tile_threads;
   pl->fcfb_ctas_per_sm = ctas_per_sm;
   pl->persist_grid = pl->sms * ctas_per_sm;
@@ -843,8 +871,9 @@ int sk_plan_set_tuning(sk_plan* pl, int32_t tile_threads, int32_t ctas_per_sm) {
   return SK_OK;
 }
 
-int sk_plan_get_tuning(const sk_plan* pl, int32_t* tile_threads, int32_t* ctas_per_sm) {
-  if (check_plan(pl) || !tile_threads || !ctas_per_sm) return fail(SK_ERR_ARG, "null argument");
+int sk_plan_get_tuning(const sk_plan* pl, int32_t* tile_size, int32_t* tile_threads, int32_t* ctas_per_sm) {
+  if (check_plan(pl) || !tile_size || !tile_threads || !ctas_per_sm) return fail(SK_ERR_ARG, "null argument");
+  *tile_size = pl->fcfb_size;
   *tile_threads = pl->fcfb_threads;
   *ctas_per_sm = pl->fcfb_ctas_per_sm;
   return SK_OK;
@@ -868,22 +897,24 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   if (cache_path) {
     if (FILE* f = fopen(cache_path, "r")) {
       char line[1024];
-      int tt = 0, cps = 0;
+      int ts = 0, tt = 0, cps = 0;
       double us = 0;
       bool found = false;
       while (fgets(line, sizeof line, f)) {
         const char* k = strstr(line, "\"key\": \"");
         if (!k || strncmp(k + 8, key, strlen(key)) != 0 || k[8 + strlen(key)] != '"') continue;
+        const char* z = strstr(line, "\"tile_size\": ");
         const char* a = strstr(line, "\"tile_threads\": ");
         const char* b = strstr(line, "\"ctas_per_sm\": ");
         const char* c = strstr(line, "\"us\": ");
-        if (a && b && sscanf(a + 16, "%d", &tt) == 1 && sscanf(b + 15, "%d", &cps) == 1) {
+        if (z && a && b && sscanf(z + 13, "%d", &ts) == 1 && sscanf(a + 16, "%d", &tt) == 1 &&
+            sscanf(b + 15, "%d", &cps) == 1) {
           if (c) sscanf(c + 6, "%lf", &us);
           found = true;                  // the last matching line wins
         }
       }
       fclose(f);
-      if (found && sk_plan_set_tuning(pl, tt, cps) == SK_OK) {
+      if (found && sk_plan_set_tuning(pl, ts, tt, cps) == SK_OK) {
         if (best_us) *best_us = us;
         return SK_OK;
       }
@@ -899,36 +930,41 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   cudaEvent_t e0, e1;
   SK_CUDA(cudaEventCreate(&e0));
   SK_CUDA(cudaEventCreate(&e1));
-  const int shapes[] = {256, 512};
-  int best_t = pl->fcfb_threads, best_c = pl->fcfb_ctas_per_sm;
+  const int shapes[][2] = {{8192, 256}, {8192, 512}, {4096, 256}};
+  const int size0 = pl->fcfb_size;
+  int best_s = pl->fcfb_size, best_t = pl->fcfb_threads, best_c = pl->fcfb_ctas_per_sm;
   float best = 1e30f;
-  for (int tt : shapes) {
+  for (const auto& sh : shapes) {
     int max_per_sm = 0;
-    if (fcfb_occupancy(tt, &max_per_sm) != cudaSuccess) continue;
+    if (fcfb_occupancy(sh[0], sh[1], &max_per_sm) != cudaSuccess) continue;
+    pl->fcfb_size = sh[0];                  // selects the shape's work list for fcfb_args
+    const int ntiles = cur_tiles(pl).n_batched;
     for (int cps = 1; cps <= max_per_sm; ++cps) {
       FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, pl->d_X);
-      const int grid = std::min(pl->sms * cps, pl->n_batched_tiles);
+      const int grid = std::min(pl->sms * cps, ntiles);
       float ms = 0.f;
       for (int it = 0; it < 7; ++it) {
         if (it == 2) SK_CUDA(cudaEventRecord(e0, st));
         SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
-        SK_CUDA(launch_fcfb(pl->cplx, true, tt, grid, a, 0, st));
+        SK_CUDA(launch_fcfb(pl->cplx, true, sh[0], sh[1], grid, a, 0, st));
       }
       SK_CUDA(cudaEventRecord(e1, st));
       SK_CUDA(cudaEventSynchronize(e1));
       SK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best) { best = ms; best_t = tt; best_c = cps; }
+      if (ms < best) { best = ms; best_s = sh[0]; best_t = sh[1]; best_c = cps; }
     }
   }
+  pl->fcfb_size = size0;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  const int rc = sk_plan_set_tuning(pl, best_t, best_c);
+  const int rc = sk_plan_set_tuning(pl, best_s, best_t, best_c);
   if (rc) return rc;
   const double us = best * 1000.0 / 5.0;
   if (best_us) *best_us = us;
   if (cache_path) {
     if (FILE* f = fopen(cache_path, "a")) {
-      fprintf(f, "{\"key\": \"%s\", \"tile_threads\": %d, \"ctas_per_sm\": %d, \"us\": %.3f}\n", key, best_t, best_c, us);
+      fprintf(f, "{\"key\": \"%s\", \"tile_size\": %d, \"tile_threads\": %d, \"ctas_per_sm\": %d, \"us\": %.3f}\n", key,
+              best_s, best_t, best_c, us);
       fclose(f);
     }
   }

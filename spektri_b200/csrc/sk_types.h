@@ -78,7 +78,7 @@ struct FcfbArgs {
   const ChanDev* chans;
   const float2* X;             // [B][K]
   int K, log2N;
-  const float2* tw;            // W_S^k
+  const float2* tw;            // W_8192^k, k < 8192
 };
 
 struct BwdArgs {
@@ -110,11 +110,14 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st);
 cudaError_t fcfb_prepare();
-// Filter-bank tile shapes: tile_threads = 256 (32 elements per thread) or 512 (16).
-cudaError_t fcfb_occupancy(int tile_threads, int* ctas_per_sm);
-cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_threads, int grid, const FcfbArgs& a, int tile_base,
-                        cudaStream_t st);
-const void* fcfb_kernel_ptr(int tile_threads, bool cplx, bool persistent);
+// Filter-bank tile shapes (tile_size, tile_threads): (8192, 256), (8192, 512)
+// and (4096, 256); a 4096-point tile runs an 8192-point transform as two halves.
+bool fcfb_shape_ok(int tile_size, int tile_threads);
+constexpr size_t fcfb_smem(int tile_size) { return sizeof(float2) * (size_t)(tile_size + tile_size / 16); }
+cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* ctas_per_sm);
+cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
+                        int tile_base, cudaStream_t st);
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 const void* fwd_kernel_ptr(int fmt, bool col);

@@ -200,7 +200,7 @@ class Plan:
 
     def autotune(self, cache_path=None):
         """Pick the filter-bank tile shape and persistent grid by timing (or
-        from the JSON-lines cache).  Returns (tile_threads, ctas_per_sm, us)."""
+        from the JSON-lines cache).  Returns (tile_size, tile_threads, ctas_per_sm, us)."""
         if cache_path is None:
             cache_path = os.environ.get("SPEKTRI_TUNE_CACHE") or os.path.join(
                 os.path.expanduser("~"), ".cache", "spektri_b200", "tune.jsonl")
@@ -210,13 +210,16 @@ class Plan:
         check(lib().sk_plan_autotune(self._h, cache_path.encode() if cache_path else None, C.byref(us)), "sk_plan_autotune")
         return self.tuning() + (us.value,)
 
-    def set_tuning(self, tile_threads: int, ctas_per_sm: int):
-        check(lib().sk_plan_set_tuning(self._h, int(tile_threads), int(ctas_per_sm)), "sk_plan_set_tuning")
+    def set_tuning(self, tile_size: int, tile_threads: int, ctas_per_sm: int):
+        """Filter-bank tile shape: 8192 x 256, 8192 x 512 or 4096 x 256, and
+        persistent CTAs per SM."""
+        check(lib().sk_plan_set_tuning(self._h, int(tile_size), int(tile_threads), int(ctas_per_sm)),
+              "sk_plan_set_tuning")
 
     def tuning(self):
-        t, c = C.c_int32(), C.c_int32()
-        check(lib().sk_plan_get_tuning(self._h, C.byref(t), C.byref(c)))
-        return t.value, c.value
+        z, t, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().sk_plan_get_tuning(self._h, C.byref(z), C.byref(t), C.byref(c)))
+        return z.value, t.value, c.value
 
     def set_timing(self, enable: bool = True):
         check(lib().sk_plan_set_timing(self._h, int(bool(enable))))

@@ -214,14 +214,16 @@ def test_device_path_matches_host_path():
                 assert q1 == q2 and np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("shape", [(256, 1), (512, 1), (512, 2)])
-def test_tile_shapes_against_oracle(shape):
+@pytest.mark.parametrize("shape", [(8192, 256, 1), (8192, 512, 1), (8192, 512, 2), (4096, 256, 1), (4096, 256, 3)])
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_tile_shapes_against_oracle(shape, mode):
     """Every filter-bank tile shape the autotuner may pick meets the bar, for
-    every IFFT size 4..8192 (radix plans differ between the shapes)."""
+    every IFFT size 4..8192 (radix plans differ between the shapes; 4096-point
+    tiles run n = 8192 as two halves)."""
     N, B = 4096, 4
     sizes = [4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192]
     filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * (37 * i + 5)) for i, n in enumerate(sizes)]
-    plan = make_plan(N * 1000.0, N, "s16le", filters, B, 3)
+    plan = make_plan(N * 1000.0, N, "s16le", filters, B, 3, mode=mode)
     plan.set_tuning(*shape)
     assert plan.tuning() == shape
     rng = np.random.default_rng(21)
@@ -234,11 +236,11 @@ def test_autotune_picks_and_caches(tmp_path):
     plan = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages)
     cache = tmp_path / "tune.jsonl"
     t1 = plan.autotune(str(cache))
-    assert t1[0] in (256, 512) and t1[1] >= 1 and t1[2] > 0
+    assert t1[:2] in ((8192, 256), (8192, 512), (4096, 256)) and t1[2] >= 1 and t1[3] > 0
     lines = cache.read_text().splitlines()
-    assert len(lines) == 1 and '"tile_threads"' in lines[0]
+    assert len(lines) == 1 and '"tile_size"' in lines[0]
     plan2 = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, w.averages)
-    assert plan2.autotune(str(cache))[:2] == t1[:2]              # read back, not re-measured
+    assert plan2.autotune(str(cache))[:3] == t1[:3]              # read back, not re-measured
     assert len(cache.read_text().splitlines()) == 1
     raw = workloads.stream_numpy(w, 0, 2 * w.samples_per_buffer).view(np.uint8)
     run_compare(plan2, w.fmt, np.split(raw, 2))
