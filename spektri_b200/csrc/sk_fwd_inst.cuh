@@ -13,9 +13,16 @@ cudaError_t fwd_launch_one(int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Column pass: registers for R1 <= 8 (one thread per column), shared-memory
+// R1-point transforms above (grid = B * R1 tiles).
 template <int FMT>
 cudaError_t fwd_col_launch_one(int grid, const FwdArgs& a, float2* Y, cudaStream_t st) {
-  fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
+  if (a.log2R1 <= 3) {
+    const long long cols = (long long)a.B << TILE_LOGS;
+    fwd_colreg_kernel<FMT><<<(unsigned)((cols + 255) / 256), 256, 0, st>>>(a, Y);
+  } else {
+    fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
+  }
   return cudaGetLastError();
 }
 
@@ -28,9 +35,11 @@ cudaError_t fwd_prepare_one() {
                               (int)TILE_SMEM);
 }
 
+// kind 0: single-pass kernel; 1: shared-memory column pass; 2: register column pass.
 template <int FMT>
-const void* fwd_ptr_one(bool col) {
-  return col ? (const void*)fwd_col_kernel<TILE_S, TILE_T, FMT> : (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
+const void* fwd_ptr_one(int kind) {
+  if (kind == 2) return (const void*)fwd_colreg_kernel<FMT>;
+  return kind ? (const void*)fwd_col_kernel<TILE_S, TILE_T, FMT> : (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
 }
 
 }  // namespace sk

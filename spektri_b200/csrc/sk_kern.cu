@@ -24,11 +24,11 @@ cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr(int fmt, bool col) {
+const void* fwd_kernel_ptr(int fmt, int kind) {
   switch (format_bits(fmt)) {
-    case 8: return fwd_kernel_ptr_8(fmt, col);
-    case 16: return fwd_kernel_ptr_16(fmt, col);
-    case 32: return fwd_kernel_ptr_32(fmt, col);
+    case 8: return fwd_kernel_ptr_8(fmt, kind);
+    case 16: return fwd_kernel_ptr_16(fmt, kind);
+    case 32: return fwd_kernel_ptr_32(fmt, kind);
   }
   return nullptr;
 }

@@ -194,6 +194,51 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
   }
 }
 
+// Column pass for R1 = 2..8 (Nc = 16384..65536): one thread per column j2 of
+// one block, the R1-point DFT in registers, no shared memory; the same Y as
+// fwd_col_kernel.  Consecutive threads take consecutive columns, so every
+// load of row j1 and every store of row k1 is coalesced.
+template <int LOGR1, int FMT>
+__device__ __forceinline__ void fwd_cols_reg(const FwdArgs& a, const SampleSrc<FMT>& src, float2* Y, long long g) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int R1 = 1 << LOGR1, LOGS = TILE_LOGS;
+  const int b = (int)(g >> LOGS), j2 = (int)(g & ((1 << LOGS) - 1));
+  const long long p0 = (long long)b * a.hop;
+  float2 z[R1];
+#pragma unroll
+  for (int j1 = 0; j1 < R1; ++j1) {
+    const int jj = (j1 << LOGS) + j2;
+    const float2 v = src.pair(p0 + (CPLX ? jj : 2 * jj));
+    z[j1] = make_float2(v.x * a.wscale, v.y * a.wscale);
+  }
+  dft<R1, -1>(z);
+  const int shC = a.log2N - a.log2Nc;
+  float2* Yb = Y + ((size_t)b << a.log2Nc) + j2;
+  Yb[0] = z[0];
+#pragma unroll
+  for (int k1 = 1; k1 < R1; ++k1) Yb[(size_t)k1 << LOGS] = cmul(z[k1], __ldg(&a.tw_big[(j2 * k1) << shC]));
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(256) fwd_colreg_kernel(FwdArgs a, float2* Y) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
+  {  // carry, as in fwd_fft_kernel
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long ncomp = a.overlap * (CPLX ? 2 : 1);
+    const long long base = (a.nnew - a.overlap) * (CPLX ? 2 : 1);
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < ncomp; h += stride)
+      a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
+  }
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ((long long)a.B << TILE_LOGS)) return;
+  switch (a.log2R1) {
+    case 1: fwd_cols_reg<1, FMT>(a, src, Y, g); break;
+    case 2: fwd_cols_reg<2, FMT>(a, src, Y, g); break;
+    case 3: fwd_cols_reg<3, FMT>(a, src, Y, g); break;
+  }
+}
+
 template <int S, int T>
 __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* Y) {
   extern __shared__ float2 sm[];

@@ -248,10 +248,13 @@ WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
   return w;
 }
 
-// The forward FFT kernel(s): one fused kernel for R1 <= 8, else the column
-// pass into d_Y followed by the row pass into d_Z.
+// The forward FFT kernel(s): one kernel for Nc <= 8192 (whole blocks per
+// tile), else the column pass into d_Y (registers for R1 <= 8, shared memory
+// above) followed by the row pass into d_Z.
+int fwd_kind(const sk_plan* pl) { return pl->R1 == 1 ? 0 : pl->R1 > 8 ? 1 : 2; }
+
 cudaError_t launch_fwd_any(const sk_plan* pl, const FwdArgs& a, cudaStream_t st) {
-  if (pl->R1 <= 8) return launch_fwd(pl->fmt, fwd_grid(pl), a, st);
+  if (pl->R1 == 1) return launch_fwd(pl->fmt, fwd_grid(pl), a, st);
   const cudaError_t e = launch_fwd_col(pl->fmt, fwd_grid(pl), a, pl->d_Y, st);
   if (e != cudaSuccess) return e;
   return launch_fwd_rows(fwd_grid(pl), a, pl->d_Y, st);
@@ -325,7 +328,7 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     cudaGraphGetNodes(g, nullptr, &n);
     std::vector<cudaGraphNode_t> nodes(n);
     cudaGraphGetNodes(g, nodes.data(), &n);
-    const void* f_fwd = fwd_kernel_ptr(pl->fmt, pl->R1 > 8);
+    const void* f_fwd = fwd_kernel_ptr(pl->fmt, fwd_kind(pl));
     const void* f_welch = welch_kernel_ptr(pl->cplx);
     for (auto nd : nodes) {
       cudaGraphNodeType t;
@@ -345,8 +348,8 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     }
     pl->graph = g;
   } else {
-    // The forward node is fwd_fft_kernel(FwdArgs) or, for R1 > 8, the column
-    // pass fwd_col_kernel(FwdArgs, float2* Y): one pointer per parameter.
+    // The forward node is fwd_fft_kernel(FwdArgs) or, for R1 > 1, a column
+    // pass (FwdArgs, float2* Y): one pointer per parameter.
     cudaKernelNodeParams p = pl->p_fwd;
     float2* y = pl->d_Y;
     void* a1[] = {(void*)&fa, (void*)&y};
@@ -478,7 +481,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_halo[0], halo_n));
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
   TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
-  if (pl->R1 > 8) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B << pl->log2Nc));
+  if (pl->R1 > 1) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B << pl->log2Nc));
   TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->K));
   TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
   TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
@@ -607,7 +610,7 @@ int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
 int sk_launches_per_call(const sk_plan* pl) {
   if (!pl) return fail(SK_ERR_ARG, "null plan");
   const int fb = pl->ch.empty() ? 0 : (pl->p.mode == SK_MODE_BATCHED ? 1 : (int)pl->ch.size());
-  return (pl->R1 > 8 ? 3 : 2) + fb;
+  return (pl->R1 > 1 ? 3 : 2) + fb;
 }
 
 int sk_set_weights(sk_plan* pl, int32_t c, const float* w) {
@@ -891,7 +894,7 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   for (const auto& c : pl->ch) counts[c.log2n]++;
   unsigned long long h = 1469598103934665603ull;
   for (int v : counts) { h ^= (unsigned long long)v; h *= 1099511628211ull; }
-  char key[256];
+  char key[512];
   snprintf(key, sizeof key, "%s|N=%lld|complex=%d|B=%d|channels=%zu|mix=%016llx", prop.name, pl->N, (int)pl->cplx,
            pl->B, pl->ch.size(), h);
   if (cache_path) {

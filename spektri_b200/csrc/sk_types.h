@@ -100,7 +100,7 @@ cudaError_t fwd_prepare_32(int fmt);
 cudaError_t launch_fwd_8(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
 cudaError_t launch_fwd_16(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
 cudaError_t launch_fwd_32(int fmt, int grid, const FwdArgs& a, cudaStream_t st);
-// Two-pass forward FFT (R1 >= 16): column pass from the raw samples into Y,
+// Two-pass forward FFT (R1 >= 2): column pass from the raw samples into Y,
 // then the row pass from Y into Z.
 cudaError_t launch_fwd_col(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
 cudaError_t launch_fwd_col_8(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
@@ -120,10 +120,12 @@ cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_size, int tile_thre
 const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
-const void* fwd_kernel_ptr(int fmt, bool col);
-const void* fwd_kernel_ptr_8(int fmt, bool col);
-const void* fwd_kernel_ptr_16(int fmt, bool col);
-const void* fwd_kernel_ptr_32(int fmt, bool col);
+// kind 0: single-pass forward kernel; 1: shared-memory column pass (R1 >= 16);
+// 2: register column pass (R1 = 2..8).
+const void* fwd_kernel_ptr(int fmt, int kind);
+const void* fwd_kernel_ptr_8(int fmt, int kind);
+const void* fwd_kernel_ptr_16(int fmt, int kind);
+const void* fwd_kernel_ptr_32(int fmt, int kind);
 const void* welch_kernel_ptr(bool cplx);
 
 }  // namespace sk
