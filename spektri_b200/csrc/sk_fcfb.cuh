@@ -115,13 +115,16 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
   }
 }
 
-// Stages 2..: span L = 2^LOGL.  LAST: q < L, g = 0, output o = q + u L.
+// Stages 2..: span L = 2^LOGL (LOGL = 0: a first stage run from shared
+// memory, in place).  LAST: q < L, g = 0, output o = q + u L.
 template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store>
 __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   constexpr int SH = TILE_LOGS - LOGL - LOGR;            // tw is the 2^13-point table
   static_assert(NB >= 1 && SH >= 0, "bad stage");
-  auto twiddle = [&](float2* v, int j) { twiddle_powers<R, SH, DIR>(v, tw, j); };
+  auto twiddle = [&](float2* v, int j) {
+    if constexpr (LOGL > 0) twiddle_powers<R, SH, DIR>(v, tw, j);
+  };
   if constexpr (LAST) {
 #pragma unroll 1
     for (int bb = 0; bb < NB; ++bb) {
@@ -189,6 +192,56 @@ __device__ __forceinline__ void tile_pipeline(float2* sm, int count, const float
     stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, store);
     __syncthreads();
     stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, true>(sm, count, tw, store);
+  }
+}
+
+// Forward M-point FFT of load() left in shared memory in natural order, each
+// element e of a transform times H[e] in place, then the inverse M-point FFT
+// stored through store().  The inverse's first stage reads shared memory
+// (LOGL = 0), so every stage but the very last writes in place.
+template <int LOGM, int S, int T, class Load, class Store>
+__device__ __forceinline__ void tile_chirp(float2* sm, int count, const float2* __restrict__ tw, Load& load,
+                                           const float2* __restrict__ H, Store& store) {
+  using P = StagePlan<LOGM, S / T>;
+  stage_first<LOGM, 1 << P::r0, S, T, -1, false, true>(sm, count, load, store);
+  __syncthreads();
+  if constexpr (P::ns >= 2) {
+    stage_next<LOGM, 1 << P::r1, P::r0, S, T, -1, false>(sm, count, tw, store);
+    __syncthreads();
+  }
+  if constexpr (P::ns >= 3) {
+    stage_next<LOGM, 1 << P::r2, P::r0 + P::r1, S, T, -1, false>(sm, count, tw, store);
+    __syncthreads();
+  }
+  if constexpr (P::ns >= 4) {
+    stage_next<LOGM, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, -1, false>(sm, count, tw, store);
+    __syncthreads();
+  }
+#pragma unroll 4
+  for (int k = 0; k < S / T; ++k) {                     // pointwise product, element by element in place
+    const int e = threadIdx.x + k * T;
+    const int i = padx(e);
+    sm[i] = cmul(sm[i], __ldg(&H[e & ((1 << LOGM) - 1)]));
+  }
+  __syncthreads();
+  if constexpr (P::ns == 1) {
+    stage_next<LOGM, 1 << P::r0, 0, S, T, +1, true>(sm, count, tw, store);
+  } else {
+    stage_next<LOGM, 1 << P::r0, 0, S, T, +1, false>(sm, count, tw, store);
+    __syncthreads();
+    if constexpr (P::ns == 2) {
+      stage_next<LOGM, 1 << P::r1, P::r0, S, T, +1, true>(sm, count, tw, store);
+    } else if constexpr (P::ns == 3) {
+      stage_next<LOGM, 1 << P::r1, P::r0, S, T, +1, false>(sm, count, tw, store);
+      __syncthreads();
+      stage_next<LOGM, 1 << P::r2, P::r0 + P::r1, S, T, +1, true>(sm, count, tw, store);
+    } else {
+      stage_next<LOGM, 1 << P::r1, P::r0, S, T, +1, false>(sm, count, tw, store);
+      __syncthreads();
+      stage_next<LOGM, 1 << P::r2, P::r0 + P::r1, S, T, +1, false>(sm, count, tw, store);
+      __syncthreads();
+      stage_next<LOGM, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, +1, true>(sm, count, tw, store);
+    }
   }
 }
 
@@ -265,10 +318,53 @@ __device__ __forceinline__ void fcfb_tile_half(float2* sm, const TileMeta* meta,
   tile_pipeline<LOGS, S, T, +1, true>(sm, 1, c.tw, load, store);
 }
 
-template <int S, int T, bool REAL>
+// A chirp-z tile: count transforms of one size n (not a power of two).  With
+// buf the shifted, weighted input and c[i] = exp(+i pi i^2/n),
+//   y[k] = c[k] sum_i (buf[i] c[i]) conj(c[k - i])        (fcfb.rs:171-177)
+// is a convolution, done as IFFT_M(FFT_M(buf c) * H) with H the 1/M-scaled
+// transform of conj(c[d]) wrapped modulo M; only the kept outputs
+// [n/8, 7(n/8)) are formed (times c[k]) and stored.  These tiles run in a
+// kernel of their own, so the power-of-two tiles' register allocation is
+// not shaped by them.
+template <int LOGM, int S, int T, bool REAL>
+__device__ __forceinline__ void fcfb_tile_chirp(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c,
+                                                const BluDesc* __restrict__ bd) {
+  const int n = bd->n, half = n >> 1, lo = n >> 3, keep = 6 * lo;
+  const float2* __restrict__ chirp = bd->chirp;
+  const float2* __restrict__ H = bd->H;
+  auto load = [&](int t, int i) {
+    if (i >= n) return make_float2(0.f, 0.f);
+    const int j = i < n - half ? i + half : i - (n - half);  // (i + n/2) mod n, fcfb.rs:166-169
+    const int m = (meta[t].first + j) & (c.N - 1);
+    const float2 x = cmul(__ldg(&meta[t].w[j]), spectrum_bin<REAL>(meta[t].X, m, c.N, c.K));
+    return cmul(x, __ldg(&chirp[i]));
+  };
+  auto store = [&](int t, int o, float2 v) {
+    const int k = o - lo;
+    if ((unsigned)k < (unsigned)keep) meta[t].out[k] = cmul(v, __ldg(&chirp[o]));
+  };
+  tile_chirp<LOGM, S, T>(sm, count, c.tw, load, H, store);
+}
+
+template <int S, int T, bool REAL, bool CHIRP>
 __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const TileMeta* meta, int count,
-                                                   const FcfbTileConst& c) {
+                                                   const FcfbTileConst& c, const BluDesc* bd) {
   constexpr int LOGS = ilog2c(S);
+  if constexpr (CHIRP) {
+    switch (log2n - BLU_TAG) {
+      case 4: fcfb_tile_chirp<4, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 5: fcfb_tile_chirp<5, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 6: fcfb_tile_chirp<6, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 7: fcfb_tile_chirp<7, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 8: fcfb_tile_chirp<8, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 9: fcfb_tile_chirp<9, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 10: fcfb_tile_chirp<10, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 11: fcfb_tile_chirp<11, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 12: if constexpr (LOGS >= 12) fcfb_tile_chirp<12, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 13: if constexpr (LOGS >= 13) fcfb_tile_chirp<13, S, T, REAL>(sm, meta, count, c, bd); break;
+    }
+    return;
+  } else {
   if (log2n > LOGS) {
     if constexpr (LOGS < TILE_LOGS) fcfb_tile_half<S, T, REAL>(sm, meta, c);
     return;
@@ -286,6 +382,7 @@ __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const 
     case 11: fcfb_tile<11, S, T, REAL>(sm, meta, count, c); break;
     case 12: if constexpr (LOGS >= 12) fcfb_tile<12, S, T, REAL>(sm, meta, count, c); break;
     case 13: if constexpr (LOGS >= 13) fcfb_tile<13, S, T, REAL>(sm, meta, count, c); break;
+  }
   }
 }
 

@@ -73,11 +73,17 @@ cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
 #ifndef FCFB_MINB_4096
 #define FCFB_MINB_4096 4
 #endif
-template <int S, int T, int MINB>
-const void* fcfb_fn(bool cplx, bool persistent) {
+template <int S, int T, int MINB, bool CHIRP>
+const void* fcfb_fn2(bool cplx, bool persistent) {
   if (persistent)
-    return cplx ? (const void*)fcfb_kernel<S, T, MINB, true, false> : (const void*)fcfb_kernel<S, T, MINB, true, true>;
-  return cplx ? (const void*)fcfb_kernel<S, T, MINB, false, false> : (const void*)fcfb_kernel<S, T, MINB, false, true>;
+    return cplx ? (const void*)fcfb_kernel<S, T, MINB, true, false, CHIRP>
+                : (const void*)fcfb_kernel<S, T, MINB, true, true, CHIRP>;
+  return cplx ? (const void*)fcfb_kernel<S, T, MINB, false, false, CHIRP>
+              : (const void*)fcfb_kernel<S, T, MINB, false, true, CHIRP>;
+}
+template <int S, int T, int MINB>
+const void* fcfb_fn(bool cplx, bool persistent, bool chirp) {
+  return chirp ? fcfb_fn2<S, T, MINB, true>(cplx, persistent) : fcfb_fn2<S, T, MINB, false>(cplx, persistent);
 }
 
 bool fcfb_shape_ok(int tile_size, int tile_threads) {
@@ -85,16 +91,17 @@ bool fcfb_shape_ok(int tile_size, int tile_threads) {
          (tile_size == 4096 && tile_threads == 256);
 }
 
-const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent) {
-  if (tile_size == 4096) return fcfb_fn<4096, 256, FCFB_MINB_4096>(cplx, persistent);
-  return tile_threads == 512 ? fcfb_fn<TILE_S, 512, 2>(cplx, persistent) : fcfb_fn<TILE_S, TILE_T, 2>(cplx, persistent);
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp) {
+  if (tile_size == 4096) return fcfb_fn<4096, 256, FCFB_MINB_4096>(cplx, persistent, chirp);
+  return tile_threads == 512 ? fcfb_fn<TILE_S, 512, 2>(cplx, persistent, chirp)
+                             : fcfb_fn<TILE_S, TILE_T, 2>(cplx, persistent, chirp);
 }
 
 cudaError_t fcfb_prepare() {
   const int shapes[][2] = {{8192, 256}, {8192, 512}, {4096, 256}};
   for (const auto& sh : shapes)
-    for (int k = 0; k < 4; ++k) {
-      const cudaError_t e = cudaFuncSetAttribute(fcfb_kernel_ptr(sh[0], sh[1], k & 1, k & 2),
+    for (int k = 0; k < 8; ++k) {
+      const cudaError_t e = cudaFuncSetAttribute(fcfb_kernel_ptr(sh[0], sh[1], k & 1, k & 2, k & 4),
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcfb_smem(sh[0]));
       if (e != cudaSuccess) return e;
     }
@@ -109,16 +116,16 @@ cudaError_t fcfb_prepare() {
 }
 
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_size, tile_threads, false, true),
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_size, tile_threads, false, true, false),
                                                        tile_threads, fcfb_smem(tile_size));
 }
 
-cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
-                        int tile_base, cudaStream_t st) {
+cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
+                        const FcfbArgs& a, int tile_base, cudaStream_t st) {
   FcfbArgs args = a;
   int base = tile_base;
   void* params[] = {(void*)&args, (void*)&base};
-  return cudaLaunchKernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent), dim3(grid), dim3(tile_threads),
+  return cudaLaunchKernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent, chirp), dim3(grid), dim3(tile_threads),
                           params, fcfb_smem(tile_size), st);
 }
 

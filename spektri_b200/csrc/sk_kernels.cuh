@@ -372,7 +372,9 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
 }
 
 // ----------------------------------------------------------------- filter bank
-template <int S, int T, int MINB, bool PERSIST, bool REAL>
+// CHIRP: the chirp-z tiles of the list (their own launch); else the
+// power-of-two tiles.
+template <int S, int T, int MINB, bool PERSIST, bool REAL, bool CHIRP>
 __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base) {
   extern __shared__ float2 sm[];
   __shared__ TileMeta s_meta[MAX_TILE_TRANSFORMS];
@@ -400,8 +402,8 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
     if (threadIdx.x < td.count) {
       const int2 cb = __ldg(&a.list[td.list_off + threadIdx.x]);
       const ChanDev& ch = a.chans[cb.x];
-      const int keep = 6 * ((1 << td.log2n) >> 3);
-      const bool half = td.log2n > ilog2c(S);                // entry (channel, 2 block + half)
+      const int keep = 6 * ((CHIRP ? a.blu[td.pad].n : 1 << td.log2n) >> 3);
+      const bool half = !CHIRP && td.log2n > ilog2c(S);      // entry (channel, 2 block + half)
       const int b = half ? cb.y >> 1 : cb.y;
       TileMeta m;
       m.X = a.X + (size_t)b * a.K;
@@ -412,7 +414,7 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       s_meta[threadIdx.x] = m;
     }
     __syncthreads();
-    fcfb_tile_dispatch<S, T, REAL>(td.log2n, sm, s_meta, td.count, c);
+    fcfb_tile_dispatch<S, T, REAL, CHIRP>(td.log2n, sm, s_meta, td.count, c, CHIRP ? a.blu + td.pad : nullptr);
     if constexpr (PERSIST) {
       if (threadIdx.x == 0) s_tile[(it + 1) & 1] = next;
     }

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -70,7 +71,9 @@ struct sk_plan {
 
   struct Chan {
     uint32_t n = 0;
-    int log2n = 0;
+    int log2n = 0;        // power-of-two sizes; 0 for a chirp-z channel
+    int logm = 0;         // chirp-z channels: log2 of their transform size M
+    int blu = -1;         // chirp-z channels: index of their size's BluDesc
     long long first = 0;
     double fs_out = 0, fc_out = 0;
     int filter_index = 0;
@@ -90,6 +93,9 @@ struct sk_plan {
   float2* d_X = nullptr;
   float* d_acc = nullptr;
   float2* d_w = nullptr;
+  BluDesc* d_blu = nullptr;             // chirp-z sizes (one per distinct n)
+  float2* d_blu_tab = nullptr;          // their chirps and kernel spectra
+  std::vector<BluDesc> h_blu;
   ChanDev* d_chans = nullptr;
   std::vector<ChanDev> h_chans;
   std::vector<ChanDev> h_chans_uploaded;
@@ -99,11 +105,13 @@ struct sk_plan {
     int size = 0;
     TileDesc* d_tiles = nullptr;        // batched tiles first, then each channel's own (plain mode)
     int2* d_list = nullptr;             // (channel, block), or (channel, 2 block + half) for n = 2 size
-    int n_batched = 0;
+    int n_batched = 0;                  // batched tiles: chirp-z ones [0, n_chirp), then power-of-two ones
+    int n_chirp = 0;
+    bool ok = true;                     // false when a chirp-z size needs a larger tile
     std::vector<int> plain_start, plain_count;
   };
   TileSet ts[2];                        // 8192-point tiles (also the adjoint's) and 4096-point tiles
-  int* d_cursor = nullptr;
+  int* d_cursor = nullptr;              // persistent tile cursors: power-of-two, chirp-z
   int persist_grid = 1;
   int sms = 1;                          // multiprocessors of the device
   int fcfb_size = TILE_S;               // filter-bank tile shape: points per tile,
@@ -136,7 +144,8 @@ int plan_free(sk_plan* pl) {
   DeviceGuard g(pl->p.device);
   void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->ts[0].d_tiles, pl->ts[0].d_list,
-                  pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec};
+                  pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec,
+                  pl->d_blu, pl->d_blu_tab};
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
   if (pl->graph) cudaGraphDestroy(pl->graph);
   for (void* q : ptrs) if (q) cudaFree(q);
@@ -272,6 +281,62 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* 
   return SK_OK;
 }
 
+// Chirp-z transform size for IFFT size n: the smallest M = 2^logm with
+// M >= n + keep - 1, keep = 6(n/8) (the circular convolution then matches
+// the linear one on every kept output [n/8, 7(n/8))).  0 when M > 8192.
+int chirp_logm(long long n) {
+  const long long need = n + 6 * (n / 8) - 1;
+  int lm = 4;
+  while ((1ll << lm) < need) ++lm;
+  return lm <= TILE_LOGS ? lm : 0;
+}
+
+// In-place radix-2 FFT in double (host; chirp-z kernel spectra only).
+void fft_double(std::vector<std::complex<double>>& a, int sign) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t k = 0; k < len / 2; ++k) {
+      const double ang = sign * 2.0 * M_PI * (double)k / (double)len;
+      const std::complex<double> w(std::cos(ang), std::sin(ang));
+      for (size_t i = 0; i < n; i += len) {
+        const std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+      }
+    }
+  }
+}
+
+// Chirp c[i] = exp(+i pi i^2 / n) (i < n) and H = FFT_M(g) / M with
+// g[d] = conj(c[d]) for d <= 7(n/8) - 1, g[M - d] = conj(c[d]) for
+// 1 <= d <= n - 1 - n/8, zero elsewhere; appended to tab as float2.
+void chirp_tables(long long n, int logm, std::vector<float2>& tab) {
+  const long long M = 1ll << logm, lo = n / 8, kmax = lo + 6 * lo - 1, dneg = n - 1 - lo;
+  auto c = [&](long long m) {
+    const long long r = (m % (2 * n)) * (m % (2 * n)) % (2 * n);   // exp(i pi m^2/n) has period 2n in m
+    const double a = M_PI * (double)r / (double)n;
+    return std::complex<double>(std::cos(a), std::sin(a));
+  };
+  for (long long i = 0; i < n; ++i) {
+    const std::complex<double> v = c(i);
+    tab.push_back(make_float2((float)v.real(), (float)v.imag()));
+  }
+  std::vector<std::complex<double>> g((size_t)M, 0.0);
+  for (long long d = 0; d <= kmax; ++d) g[(size_t)d] = std::conj(c(d));
+  for (long long d = 1; d <= dneg; ++d) g[(size_t)(M - d)] = std::conj(c(d));
+  fft_double(g, -1);
+  for (long long k = 0; k < M; ++k) {
+    const std::complex<double> v = g[(size_t)k] / (double)M;
+    tab.push_back(make_float2((float)v.real(), (float)v.imag()));
+  }
+}
+
 const sk_plan::TileSet& cur_tiles(const sk_plan* pl) { return pl->ts[pl->fcfb_size == TILE_S ? 0 : 1]; }
 
 FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
@@ -286,7 +351,32 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
   a.K = pl->K;
   a.log2N = pl->log2N;
   a.tw = pl->d_tw_tile;
+  a.blu = pl->d_blu;
   return a;
+}
+
+// Batched: the chirp-z tiles (if any) in one persistent launch, then the
+// power-of-two tiles in another, each with its own cursor.
+cudaError_t launch_batched(sk_plan* pl, const FcfbArgs& a0, int size, int threads, int grid, cudaStream_t st) {
+  const sk_plan::TileSet& t = pl->ts[size == TILE_S ? 0 : 1];
+  cudaError_t e = cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  FcfbArgs a = a0;
+  a.tiles = t.d_tiles;
+  a.list = t.d_list;
+  if (t.n_chirp > 0) {
+    a.cursor = pl->d_cursor + 1;
+    a.ntiles = t.n_chirp;
+    e = launch_fcfb(pl->cplx, true, true, size, threads, std::min(grid, t.n_chirp), a, 0, st);
+    if (e != cudaSuccess) return e;
+  }
+  if (t.n_batched > t.n_chirp) {
+    a.cursor = pl->d_cursor;
+    a.tiles = t.d_tiles + t.n_chirp;
+    a.ntiles = t.n_batched - t.n_chirp;
+    e = launch_fcfb(pl->cplx, true, false, size, threads, std::min(grid, a.ntiles), a, 0, st);
+  }
+  return e;
 }
 
 int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
@@ -294,12 +384,11 @@ int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, c
   FcfbArgs a = fcfb_args(pl, chans, X);
   const sk_plan::TileSet& t = cur_tiles(pl);
   if (batched) {
-    SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
-    const int grid = std::min(pl->persist_grid, t.n_batched);
-    SK_CUDA(launch_fcfb(pl->cplx, true, pl->fcfb_size, pl->fcfb_threads, grid, a, 0, st));
+    SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st));
   } else {
     for (size_t c = 0; c < pl->ch.size(); ++c)
-      SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a, t.plain_start[c], st));
+      SK_CUDA(launch_fcfb(pl->cplx, false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
+                          t.plain_start[c], st));
   }
   return SK_OK;
 }
@@ -430,13 +519,17 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       fprintf(stderr, "Invalid filter parameters\n");
     } else {
       const int l2 = ilog2_exact(bins);
-      if (l2 < 2 || l2 > TILE_LOGS) {
+      const bool pow2 = l2 >= 2 && l2 <= TILE_LOGS;
+      const int lm = pow2 ? 0 : chirp_logm(bins);
+      if (!pow2 && (bins < 4 || bins % 4 != 0 || lm == 0)) {
         st = SK_ERR_UNSUPPORTED;
-        fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two 4..%d)\n", bins, S);
+        fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two up to %d, "
+                "other multiples of 4 up to 4680)\n", bins, S);
       } else {
         sk_plan::Chan c;
         c.n = (uint32_t)bins;
-        c.log2n = l2;
+        c.log2n = pow2 ? l2 : 0;
+        c.logm = lm;
         c.first = first;
         c.fs_out = filters[i].fs_out;
         c.fc_out = filters[i].fc_out;
@@ -488,7 +581,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_chans, pl->ch.size()));
   TRY(dev_alloc(&pl->d_chans_aux, pl->ch.size()));
   TRY(dev_alloc(&pl->d_bwd, pl->ch.size()));
-  TRY(dev_alloc(&pl->d_cursor, 1));
+  TRY(dev_alloc(&pl->d_cursor, 2));
   TRY(dev_alloc(&pl->d_raw, pl->raw_bytes));
   TRY(dev_alloc(&pl->d_out, pl->out_total));
   TRY(dev_alloc(&pl->d_spec, (size_t)pl->max_spectra * pl->K * pl->spec_bin_bytes));
@@ -500,6 +593,36 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   CUDA_TRY(cudaMemset(pl->d_acc, 0, sizeof(float) * pl->K));
   if (!pl->w_host.empty())
     CUDA_TRY(cudaMemcpy(pl->d_w, pl->w_host.data(), sizeof(float) * pl->w_host.size(), cudaMemcpyHostToDevice));
+
+  // Chirp-z sizes: one chirp + kernel spectrum per distinct n.
+  {
+    std::vector<float2> tab;
+    std::vector<size_t> offs;
+    for (auto& c : pl->ch) {
+      if (c.log2n) continue;
+      for (size_t k = 0; k < pl->h_blu.size(); ++k)
+        if (pl->h_blu[k].n == (int)c.n) c.blu = (int)k;
+      if (c.blu < 0) {
+        c.blu = (int)pl->h_blu.size();
+        BluDesc d{};
+        d.n = (int)c.n;
+        d.logm = c.logm;
+        pl->h_blu.push_back(d);
+        offs.push_back(tab.size());
+        chirp_tables(c.n, c.logm, tab);
+      }
+    }
+    if (!pl->h_blu.empty()) {
+      TRY(dev_alloc(&pl->d_blu_tab, tab.size()));
+      TRY(dev_alloc(&pl->d_blu, pl->h_blu.size()));
+      CUDA_TRY(cudaMemcpy(pl->d_blu_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
+      for (size_t k = 0; k < pl->h_blu.size(); ++k) {
+        pl->h_blu[k].chirp = pl->d_blu_tab + offs[k];
+        pl->h_blu[k].H = pl->d_blu_tab + offs[k] + pl->h_blu[k].n;
+      }
+      CUDA_TRY(cudaMemcpy(pl->d_blu, pl->h_blu.data(), sizeof(BluDesc) * pl->h_blu.size(), cudaMemcpyHostToDevice));
+    }
+  }
 
   // Channel table (output pointers start at the plan's own buffer).
   pl->h_chans.resize(pl->ch.size());
@@ -536,6 +659,19 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
         }
     };
     auto per_tile = [&](int l2) { return l2 > logt ? 1 : std::min(t.size >> l2, MAX_TILE_TRANSFORMS); };
+    // chirp-z sizes first (the most work per point), largest transform first
+    for (int lm = TILE_LOGS; lm >= 4; --lm)
+      for (size_t k = 0; k < pl->h_blu.size(); ++k) {
+        if (pl->h_blu[k].logm != lm) continue;
+        if (lm > logt) { t.ok = false; continue; }
+        const int base = (int)list.size();
+        for (size_t c = 0; c < pl->ch.size(); ++c)
+          if (pl->ch[c].blu == (int)k) add((int)c, 0);
+        const int cnt = (int)list.size() - base, per = std::min(t.size >> lm, MAX_TILE_TRANSFORMS);
+        for (int o = 0; o < cnt; o += per)
+          tiles.push_back(TileDesc{BLU_TAG + lm, base + o, std::min(per, cnt - o), (int)k});
+      }
+    t.n_chirp = (int)tiles.size();
     for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
       const int base = (int)list.size();
       for (size_t c = 0; c < pl->ch.size(); ++c)
@@ -545,12 +681,17 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     }
     t.n_batched = (int)tiles.size();
     for (size_t c = 0; c < pl->ch.size(); ++c) {
-      const int l2 = pl->ch[c].log2n, per = per_tile(l2);
+      const sk_plan::Chan& ch = pl->ch[c];
+      const bool chirp = ch.log2n == 0;
+      const int l2 = chirp ? 0 : ch.log2n;
+      const int per = chirp ? std::max(1, std::min(t.size >> std::min(ch.logm, logt), MAX_TILE_TRANSFORMS)) : per_tile(l2);
       const int base = (int)list.size();
       add((int)c, l2);
       const int cnt = (int)list.size() - base;
       t.plain_start.push_back((int)tiles.size());
-      for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
+      for (int o = 0; o < cnt; o += per)
+        tiles.push_back(chirp ? TileDesc{BLU_TAG + ch.logm, base + o, std::min(per, cnt - o), ch.blu}
+                              : TileDesc{l2, base + o, std::min(per, cnt - o), 0});
       t.plain_count.push_back((int)tiles.size() - t.plain_start.back());
     }
     TRY(dev_alloc(&t.d_list, list.size()));
@@ -609,7 +750,8 @@ int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
 
 int sk_launches_per_call(const sk_plan* pl) {
   if (!pl) return fail(SK_ERR_ARG, "null plan");
-  const int fb = pl->ch.empty() ? 0 : (pl->p.mode == SK_MODE_BATCHED ? 1 : (int)pl->ch.size());
+  const int fb = pl->ch.empty() ? 0
+                 : (pl->p.mode == SK_MODE_BATCHED ? 1 + (pl->h_blu.empty() ? 0 : 1) : (int)pl->ch.size());
   return (pl->R1 > 1 ? 3 : 2) + fb;
 }
 
@@ -783,7 +925,11 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   }
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
-  SK_CUDA(launch_fcfb(pl->cplx, false, pl->fcfb_size, pl->fcfb_threads, cur_tiles(pl).n_batched, a, 0, st));
+  const sk_plan::TileSet& t = cur_tiles(pl);
+  if (t.n_chirp > 0) SK_CUDA(launch_fcfb(pl->cplx, false, true, pl->fcfb_size, pl->fcfb_threads, t.n_chirp, a, 0, st));
+  if (t.n_batched > t.n_chirp)
+    SK_CUDA(launch_fcfb(pl->cplx, false, false, pl->fcfb_size, pl->fcfb_threads, t.n_batched - t.n_chirp, a,
+                        t.n_chirp, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
@@ -792,6 +938,8 @@ int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, 
                             float* const* dW, float* dX, void* stream) {
   if (check_plan(pl)) return SK_ERR_ARG;
   if (!X || (!pl->ch.empty() && (!W || !dy || !dW))) return fail(SK_ERR_ARG, "null argument");
+  if (!pl->h_blu.empty())
+    return fail(SK_ERR_UNSUPPORTED, "the adjoint covers power-of-two IFFT sizes; this plan has chirp-z channels");
   DeviceGuard g(pl->p.device);
   cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
   std::vector<BwdChan> bc(pl->ch.size());
@@ -854,6 +1002,8 @@ int sk_plan_set_tuning(sk_plan* pl, int32_t tile_size, int32_t tile_threads, int
   if (check_plan(pl)) return SK_ERR_ARG;
   if (!fcfb_shape_ok(tile_size, tile_threads))
     return fail(SK_ERR_ARG, "tile shape %d x %d: use 8192 x 256, 8192 x 512 or 4096 x 256", tile_size, tile_threads);
+  if (!pl->ts[tile_size == TILE_S ? 0 : 1].ok)
+    return fail(SK_ERR_ARG, "tile size %d is smaller than a chirp-z transform of this plan", tile_size);
   DeviceGuard g(pl->p.device);
   int max_per_sm = 0;
   SK_CUDA(fcfb_occupancy(tile_size, tile_threads, &max_per_sm));
@@ -894,6 +1044,8 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   for (const auto& c : pl->ch) counts[c.log2n]++;
   unsigned long long h = 1469598103934665603ull;
   for (int v : counts) { h ^= (unsigned long long)v; h *= 1099511628211ull; }
+  for (const auto& c : pl->ch)             // chirp-z sizes enter by value
+    if (!c.log2n) { h ^= (unsigned long long)c.n; h *= 1099511628211ull; }
   char key[512];
   snprintf(key, sizeof key, "%s|N=%lld|complex=%d|B=%d|channels=%zu|mix=%016llx", prop.name, pl->N, (int)pl->cplx,
            pl->B, pl->ch.size(), h);
@@ -939,6 +1091,7 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   float best = 1e30f;
   for (const auto& sh : shapes) {
     int max_per_sm = 0;
+    if (!pl->ts[sh[0] == TILE_S ? 0 : 1].ok) continue;
     if (fcfb_occupancy(sh[0], sh[1], &max_per_sm) != cudaSuccess) continue;
     pl->fcfb_size = sh[0];                  // selects the shape's work list for fcfb_args
     const int ntiles = cur_tiles(pl).n_batched;
@@ -948,8 +1101,7 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
       float ms = 0.f;
       for (int it = 0; it < 7; ++it) {
         if (it == 2) SK_CUDA(cudaEventRecord(e0, st));
-        SK_CUDA(cudaMemsetAsync(pl->d_cursor, 0, sizeof(int), st));
-        SK_CUDA(launch_fcfb(pl->cplx, true, sh[0], sh[1], grid, a, 0, st));
+        SK_CUDA(launch_batched(pl, a, sh[0], sh[1], grid, st));
       }
       SK_CUDA(cudaEventRecord(e1, st));
       SK_CUDA(cudaEventSynchronize(e1));

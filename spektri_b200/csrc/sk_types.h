@@ -34,11 +34,22 @@ struct BwdChan {
   int pad;
 };
 struct TileDesc {              // transforms of one size
-  int log2n;
+  int log2n;                   // log2 n, or BLU_TAG + log2 M for a chirp-z tile
   int list_off;                // first entry in the (channel, block) list
   int count;                   // transforms in this tile
-  int pad;
+  int pad;                     // chirp-z tiles: index of their BluDesc
 };
+
+// Chirp-z (Bluestein) channels: an IFFT size n that is a multiple of 4 but
+// not a power of two runs as a forward and an inverse M-point FFT, M = 2^logm
+// the smallest power of two >= n + 6(n/8) - 1 (what the kept outputs
+// [n/8, 7(n/8)) need of the circular convolution).
+struct BluDesc {
+  const float2* chirp;         // c[i] = exp(+i pi i^2 / n), i < n
+  const float2* H;             // forward M-point FFT of the kernel conj(c[d]) (d wrapped mod M), times 1/M
+  int n, logm;
+};
+constexpr int BLU_TAG = 16;
 
 struct FwdArgs {
   const uint8_t* raw;          // new samples of this buffer
@@ -79,6 +90,7 @@ struct FcfbArgs {
   const float2* X;             // [B][K]
   int K, log2N;
   const float2* tw;            // W_8192^k, k < 8192
+  const BluDesc* blu;          // chirp-z sizes (may be null)
 };
 
 struct BwdArgs {
@@ -115,9 +127,10 @@ cudaError_t fcfb_prepare();
 bool fcfb_shape_ok(int tile_size, int tile_threads);
 constexpr size_t fcfb_smem(int tile_size) { return sizeof(float2) * (size_t)(tile_size + tile_size / 16); }
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* ctas_per_sm);
-cudaError_t launch_fcfb(bool cplx, bool persistent, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
-                        int tile_base, cudaStream_t st);
-const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent);
+// chirp: the kernel for chirp-z tiles (else power-of-two tiles).
+cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
+                        const FcfbArgs& a, int tile_base, cudaStream_t st);
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 // kind 0: single-pass forward kernel; 1: shared-memory column pass (R1 >= 16);

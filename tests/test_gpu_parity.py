@@ -128,16 +128,17 @@ def test_edge_channels_wrap_mirror_and_drops():
         dict(fs_out=8192e3, fc_out=1000e3),             # n = 8192 > N: wraps more than once
         dict(fs_out=4e3, fc_out=100e3),                 # n = 4
         dict(fs_out=64e3, fc_out=1001e3),               # centre not a multiple of 4: dropped
-        dict(fs_out=48e3, fc_out=0.0),                  # n = 48: exact, but not a power of two
+        dict(fs_out=48e3, fc_out=0.0),                  # n = 48: not a power of two (chirp-z)
         dict(fs_out=-4e3, fc_out=0.0),                  # bins <= 0: dropped
+        dict(fs_out=4684e3, fc_out=0.0),                # n = 4684: beyond the device's chirp-z sizes
     ]
     plan = make_plan(fs, N, "s16le", filters, B, 5)
-    assert plan.filter_status[:4] == [0, 0, 0, 0]
+    assert plan.filter_status[:4] == [0, 0, 0, 0] and plan.filter_status[5] == 0
     assert plan.filter_status[4] == SK_ERR_FILTER and plan.filter_status[6] == SK_ERR_FILTER
-    assert plan.filter_status[5] == SK_ERR_UNSUPPORTED
-    o32 = oracle32.Oracle32(fs, 0.0, N, B, 5, "s16le", filters)
+    assert plan.filter_status[7] == SK_ERR_UNSUPPORTED
+    o32 = oracle32.Oracle32(fs, 0.0, N, B, 5, "s16le", filters[:7])
     assert o32.filter_status[4] != 0 and o32.filter_status[6] != 0 and o32.filter_status[5] == 0
-    assert [(c["bins"], c["first"]) for c in plan.channels] == [o32.channels[i] for i in (0, 1, 2, 3)]
+    assert [(c["bins"], c["first"]) for c in plan.channels] == [o32.channels[i] for i in (0, 1, 2, 3, 4)]
     rng = np.random.default_rng(11)
     from tests.test_oracle import _stream
     run_compare(plan, "s16le", [_stream("s16le", plan.new_samples, rng) for _ in range(4)])
@@ -365,3 +366,43 @@ def test_carry_starts_mid_stream(fmt, mode):
                     assert np.array_equal(a, r)
     with pytest.raises(ValueError):
         p0.set_carry(np.zeros(3, np.uint8))
+
+
+CHIRP_SIZES = [12, 20, 28, 36, 100, 300, 1000, 1012, 2340]
+CHIRP_SIZES_BIG = [3000, 4036, 4680]                    # chirp-z transforms of 8192 points
+
+
+@pytest.mark.parametrize("fmt", ["s16le", "cf32le"])
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+@pytest.mark.parametrize("shape", [(8192, 256, 2), (4096, 256, 4)])
+def test_chirp_sizes_against_oracle(fmt, mode, shape):
+    """IFFT sizes that are multiples of 4 but not powers of two (the reference
+    plans any size, fcfb.rs:150) run as chirp-z transforms; mixed with
+    power-of-two channels in one plan, they meet the same bar."""
+    N, B = 4096, 4
+    cplx = oracle64.is_complex(fmt)
+    sizes = CHIRP_SIZES + (CHIRP_SIZES_BIG if shape[0] == 8192 else []) + [64, 8192]
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * ((-1) ** i * (53 * i + 3) if cplx else 53 * i + 3))
+               for i, n in enumerate(sizes)]
+    plan = make_plan(N * 1000.0, N, fmt, filters, B, 3, mode=mode)
+    assert [c["bins"] for c in plan.channels] == sizes
+    plan.set_tuning(*shape)
+    rng = np.random.default_rng(31)
+    from tests.test_oracle import _stream
+    worst = run_compare(plan, fmt, [_stream(fmt, plan.new_samples, rng) for _ in range(3)])
+    print(f"chirp {fmt} {mode} {shape}: worst rel rms {worst:.2e}")
+
+
+def test_chirp_limits():
+    """Sizes whose chirp-z transform exceeds 8192 points are dropped with a
+    status; a 4096-point tile shape is refused while a plan holds a chirp-z
+    size that needs 8192 points."""
+    N = 4096
+    filters = [dict(fs_out=1000.0 * n, fc_out=0.0) for n in (4680, 4684, 12)]
+    plan = make_plan(N * 1000.0, N, "s16le", filters, 4, 3)
+    assert plan.filter_status == [0, SK_ERR_UNSUPPORTED, 0]
+    assert [c["bins"] for c in plan.channels] == [4680, 12]
+    with pytest.raises(SpektriError):
+        plan.set_tuning(4096, 256, 1)
+    plan.set_tuning(8192, 256, 1)
+    assert plan.autotune("")[0] == 8192                          # no cache file
