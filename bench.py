@@ -281,6 +281,20 @@ def main():
     hbm, peak_kind = peaks()
     achieved = out_bytes / (fcfb_ms / 1e3) / 1e9
     alg = w.alg_bytes_per_sample()
+    # FP32 work of the same launch: per block and channel an n-point complex
+    # FFT (5 n log2 n) plus the weight product (6 n); chirp-z sizes count two
+    # M-point FFTs and three pointwise products.
+    flops = 0.0
+    for c in plan.channels:
+        n = c["bins"]
+        if n & (n - 1) == 0:
+            flops += 5.0 * n * math.log2(n) + 6.0 * n
+        else:
+            m = 1 << math.ceil(math.log2(n + 6 * (n // 8) - 1))
+            flops += 2 * 5.0 * m * math.log2(m) + 18.0 * m
+    flops *= w.ffts_per_buf
+    props = torch.cuda.get_device_properties(dev)
+    fp32_peak = props.multi_processor_count * 128 * 2 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
     result = {
         "metric": "input Msamples/s", "value": round(value, 2), "unit": "Msamples/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
@@ -300,7 +314,10 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "fcfb_kernel (persistent)", "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "peak_kind": f"{peak_kind} copy bandwidth", "traffic": None,
-                     "alg_bytes_per_launch": out_bytes, "launch_ms": round(fcfb_ms, 4)},
+                     "alg_bytes_per_launch": out_bytes, "launch_ms": round(fcfb_ms, 4),
+                     "fp32": {"flop_per_launch": round(flops), "achieved_tflops": round(flops / (fcfb_ms / 1e3) / 1e12, 2),
+                              "peak_tflops": round(fp32_peak, 1), "frac": round(flops / (fcfb_ms / 1e3) / 1e12 / fp32_peak, 4),
+                              "peak_kind": "SMs x 128 FP32 lanes x 2 x max SM clock"}},
         "gpu_launches": plan.launches_per_call * args.steps,
         "clocks": clk,
     }
