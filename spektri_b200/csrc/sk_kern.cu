@@ -69,22 +69,8 @@ cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
 // Filter-bank tile shapes (tile size x threads, minimum CTAs per SM):
 // 8192 x 256 (32 elements per thread, 2 CTAs/SM), 8192 x 512 (16 elements,
 // radix <= 16 stages, 2 CTAs/SM), 4096 x 256 (16 elements, n = 8192 as two
-// independent halves, FCFB_MINB_4096 CTAs/SM).
-#ifndef FCFB_MINB_4096
-#define FCFB_MINB_4096 4
-#endif
-template <int S, int T, int MINB, bool CHIRP>
-const void* fcfb_fn2(bool cplx, bool persistent) {
-  if (persistent)
-    return cplx ? (const void*)fcfb_kernel<S, T, MINB, true, false, CHIRP>
-                : (const void*)fcfb_kernel<S, T, MINB, true, true, CHIRP>;
-  return cplx ? (const void*)fcfb_kernel<S, T, MINB, false, false, CHIRP>
-              : (const void*)fcfb_kernel<S, T, MINB, false, true, CHIRP>;
-}
-template <int S, int T, int MINB>
-const void* fcfb_fn(bool cplx, bool persistent, bool chirp) {
-  return chirp ? fcfb_fn2<S, T, MINB, true>(cplx, persistent) : fcfb_fn2<S, T, MINB, false>(cplx, persistent);
-}
+// independent halves, 4 CTAs/SM).
+// The instances live in sk_fcfb_<shape>[_chirp].cu, compiled in parallel.
 
 bool fcfb_shape_ok(int tile_size, int tile_threads) {
   return (tile_size == 8192 && (tile_threads == 256 || tile_threads == 512)) ||
@@ -92,9 +78,11 @@ bool fcfb_shape_ok(int tile_size, int tile_threads) {
 }
 
 const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp) {
-  if (tile_size == 4096) return fcfb_fn<4096, 256, FCFB_MINB_4096>(cplx, persistent, chirp);
-  return tile_threads == 512 ? fcfb_fn<TILE_S, 512, 2>(cplx, persistent, chirp)
-                             : fcfb_fn<TILE_S, TILE_T, 2>(cplx, persistent, chirp);
+  if (tile_size == 4096)
+    return chirp ? fcfb_ptr_4096_chirp(cplx, persistent) : fcfb_ptr_4096(cplx, persistent);
+  if (tile_threads == 512)
+    return chirp ? fcfb_ptr_8192x512_chirp(cplx, persistent) : fcfb_ptr_8192x512(cplx, persistent);
+  return chirp ? fcfb_ptr_8192_chirp(cplx, persistent) : fcfb_ptr_8192(cplx, persistent);
 }
 
 cudaError_t fcfb_prepare() {

@@ -131,6 +131,13 @@ cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* ctas_per_sm);
 cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
                         const FcfbArgs& a, int tile_base, cudaStream_t st);
 const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp);
+// Per-shape instance tables (sk_fcfb_*.cu).
+const void* fcfb_ptr_8192(bool cplx, bool persistent);
+const void* fcfb_ptr_8192_chirp(bool cplx, bool persistent);
+const void* fcfb_ptr_8192x512(bool cplx, bool persistent);
+const void* fcfb_ptr_8192x512_chirp(bool cplx, bool persistent);
+const void* fcfb_ptr_4096(bool cplx, bool persistent);
+const void* fcfb_ptr_4096_chirp(bool cplx, bool persistent);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 // kind 0: single-pass forward kernel; 1: shared-memory column pass (R1 >= 16);
