@@ -13,12 +13,15 @@
 // --mode=plain|batched (default batched), --device=N and
 // --fake-clock=<secs>,<step_ns> (deterministic timestamps for tests).
 #include <cerrno>
+#include <condition_variable>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <strings.h>
 #include <unistd.h>
 #include <vector>
@@ -229,53 +232,125 @@ int main(int argc, char** argv) {
   uint8_t spec_topic[24];
   sk_spectrum_topic(spec_topic, p.spectrum_format, p.fs_in / (double)p.fft_size, p.fc_in);   // spectrum.rs:57-65
 
-  // Pinned staging: raw input, one record buffer per channel (24-byte header
-  // then payload), spectrum payloads.
+  // Three pipelined stages over a ring of pinned slots, so reading stdin,
+  // the GPU call (copy in, process, copy out) and the output I/O of
+  // consecutive buffers overlap; records still leave in buffer order.  A slot
+  // holds the raw input, one record buffer per channel (24-byte header then
+  // payload) and the spectrum payloads.
   const int bps = sk_format_bytes(fmt);
-  uint8_t* raw = (uint8_t*)sk_host_alloc(info.new_samples * (size_t)bps);
-  std::vector<uint8_t*> rec(info.n_channels);
-  std::vector<void*> payload(info.n_channels);
-  for (uint32_t c = 0; c < info.n_channels; ++c) {
-    rec[c] = (uint8_t*)sk_host_alloc(32 + outs[c].n * 8);
-    payload[c] = rec[c] + 32;   // 16-byte aligned payload; the header goes at +8
-  }
-  uint8_t* spec = (uint8_t*)sk_host_alloc((size_t)info.max_spectra * info.spectrum_bytes);
-  std::vector<uint8_t> srec(24 + info.spectrum_bytes);
-  if (!raw || !spec) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
-
-  uint64_t seq = 0;
   const size_t raw_bytes = info.new_samples * (size_t)bps;
-  while (read_exact(raw, raw_bytes)) {        // main.rs:176-178: a short read ends the stream
-    uint64_t secs = 0;
-    uint32_t nanos = 0;
-    if (fake) {
-      const unsigned long long t = clk_secs * 1000000000ull + seq * clk_step;
-      secs = t / 1000000000ull;
-      nanos = (uint32_t)(t % 1000000000ull);
-    } else {
-      timespec ts;
-      clock_gettime(CLOCK_REALTIME, &ts);   // main.rs:180
-      secs = (uint64_t)ts.tv_sec;
-      nanos = (uint32_t)ts.tv_nsec;
-    }
+  constexpr int NSLOT = 3;
+  struct Slot {
+    uint8_t* raw = nullptr;
+    std::vector<uint8_t*> rec;
+    std::vector<void*> payload;
+    uint8_t* spec = nullptr;
     sk_result r{};
-    rc = sk_process(plan, raw, payload.data(), spec, &r);
-    if (rc < 0) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
-    for (uint32_t s = 0; s < r.n_spectra; ++s) {
-      sk_serialize_metadata(srec.data(), r.spectrum_seq0 + s, secs, nanos);
-      std::memcpy(srec.data() + 24, spec + (size_t)s * info.spectrum_bytes, info.spectrum_bytes);
-      zmq.send2(spec_topic, 24, srec.data(), srec.size());
-      write_all(stdout, srec.data(), srec.size());
-    }
+    uint64_t seq = 0, secs = 0;
+    uint32_t nanos = 0;
+    int state = 0;        // 0 free, 1 read, 2 processed, 3 end of stream
+  } slots[NSLOT];
+  for (auto& sl : slots) {
+    sl.raw = (uint8_t*)sk_host_alloc(raw_bytes);
+    sl.rec.resize(info.n_channels);
+    sl.payload.resize(info.n_channels);
     for (uint32_t c = 0; c < info.n_channels; ++c) {
-      uint8_t* h = rec[c] + 8;
-      sk_serialize_metadata(h, seq, secs, nanos);     // fcfb.rs:84: seq of the buffer
-      const size_t len = 24 + outs[c].n * 8;
-      zmq.send2(outs[c].topic, 24, h, len);
-      write_all(outs[c].file, h, len);
+      sl.rec[c] = (uint8_t*)sk_host_alloc(32 + outs[c].n * 8);
+      if (!sl.rec[c]) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
+      sl.payload[c] = sl.rec[c] + 32;   // 16-byte aligned payload; the header goes at +8
     }
-    ++seq;
+    sl.spec = (uint8_t*)sk_host_alloc((size_t)info.max_spectra * info.spectrum_bytes);
+    if (!sl.raw || !sl.spec) { fprintf(stderr, "spektri: %s\n", sk_last_error()); return 1; }
   }
+  std::mutex mu;
+  std::condition_variable cv;
+  bool failed = false;
+  auto wait_state = [&](Slot& sl, int want) {
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return failed || sl.state == want || (want == 1 && sl.state == 3); });
+    return !failed;
+  };
+  auto set_state = [&](Slot& sl, int st) {
+    { std::lock_guard<std::mutex> lk(mu); sl.state = st; }
+    cv.notify_all();
+  };
+
+  // Stage 1: stdin (main.rs:176-178: a short read ends the stream).
+  std::thread reader([&] {
+    for (uint64_t seq = 0;; ++seq) {
+      Slot& sl = slots[seq % NSLOT];
+      if (!wait_state(sl, 0)) return;
+      if (!read_exact(sl.raw, raw_bytes)) { set_state(sl, 3); return; }
+      sl.seq = seq;
+      if (fake) {
+        const unsigned long long t = clk_secs * 1000000000ull + seq * clk_step;
+        sl.secs = t / 1000000000ull;
+        sl.nanos = (uint32_t)(t % 1000000000ull);
+      } else {
+        timespec ts;
+        clock_gettime(CLOCK_REALTIME, &ts);   // main.rs:180
+        sl.secs = (uint64_t)ts.tv_sec;
+        sl.nanos = (uint32_t)ts.tv_nsec;
+      }
+      set_state(sl, 1);
+    }
+  });
+  // Stage 3: framing and output, in buffer order.
+  uint8_t spec_topic_copy[24];
+  std::memcpy(spec_topic_copy, spec_topic, 24);
+  std::thread writer([&] {
+    std::vector<uint8_t> srec(24 + info.spectrum_bytes);
+    for (uint64_t k = 0;; ++k) {
+      Slot& sl = slots[k % NSLOT];
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return failed || sl.state == 2 || sl.state == 3; });
+        if (failed || sl.state == 3) return;
+      }
+      for (uint32_t s = 0; s < sl.r.n_spectra; ++s) {
+        sk_serialize_metadata(srec.data(), sl.r.spectrum_seq0 + s, sl.secs, sl.nanos);
+        std::memcpy(srec.data() + 24, sl.spec + (size_t)s * info.spectrum_bytes, info.spectrum_bytes);
+        zmq.send2(spec_topic_copy, 24, srec.data(), srec.size());
+        write_all(stdout, srec.data(), srec.size());
+      }
+      for (uint32_t c = 0; c < info.n_channels; ++c) {
+        uint8_t* h = sl.rec[c] + 8;
+        sk_serialize_metadata(h, sl.seq, sl.secs, sl.nanos);     // fcfb.rs:84: seq of the buffer
+        const size_t len = 24 + outs[c].n * 8;
+        zmq.send2(outs[c].topic, 24, h, len);
+        write_all(outs[c].file, h, len);
+      }
+      set_state(sl, 0);
+    }
+  });
+  // Stage 2: the GPU call.
+  int exit_code = 0;
+  for (uint64_t k = 0;; ++k) {
+    Slot& sl = slots[k % NSLOT];
+    if (!wait_state(sl, 1)) break;
+    if (sl.state == 3) {
+      // end of stream: let the writer drain and stop at this slot
+      std::unique_lock<std::mutex> lk(mu);
+      cv.notify_all();
+      break;
+    }
+    rc = sk_process(plan, sl.raw, sl.payload.data(), sl.spec, &sl.r);
+    if (rc < 0) {
+      fprintf(stderr, "spektri: %s\n", sk_last_error());
+      exit_code = 1;
+      { std::lock_guard<std::mutex> lk(mu); failed = true; }
+      cv.notify_all();
+      break;
+    }
+    set_state(sl, 2);
+  }
+  if (exit_code) {
+    // stdin may still block the reader: leave without joining it
+    fflush(stdout);
+    _exit(exit_code);
+  }
+  writer.join();
+  reader.join();
   fflush(stdout);
   for (auto& o : outs)
     if (o.file) fclose(o.file);

@@ -156,3 +156,33 @@ def test_host_binary_error_behaviour(tmp_path):
     r = subprocess.run([HOST, "-s", "1024000", "-n", "1024", "-I", "s16le", addr], input=b"", capture_output=True,
                        env=env, timeout=120)
     assert r.returncode == 0 and r.stdout == b""
+
+
+def test_host_binary_streams_c3(tmp_path):
+    """The pipelined binary on the batching configuration (N = 65536, 256
+    channels, B = 64): stdin, GPU call and output overlap; every buffer's
+    spectrum records arrive on stdout and the run's throughput is printed
+    (two stream lengths, so start-up cancels)."""
+    assert os.path.exists(HOST), "build spektri_b200/bin/spektri first"
+    w = workloads.c3()
+    filt = [f"fs={f['fs_out']:.17g}:fc={f['fc_out']:.17g}:tw={f.get('transition', 0)}" for f in w.filters()]
+    args = [HOST, f"--samplerate={w.fs:.17g}", f"--centerfreq={w.fc:.17g}", "-n", str(w.fft_size), "--fftbuf",
+            str(w.ffts_per_buf), f"--averages={w.averages}", "-I", "s16le", "--spectrumformat=u8",
+            f"--zmqbind=ipc://{tmp_path}/sk.zmq", "--filters"] + filt
+    env = dict(os.environ, SPEKTRI_LIBZMQ=libzmq_path())         # a PUB socket with no subscriber
+    times = {}
+    rng = np.random.default_rng(3)
+    for nbuf in (4, 20):
+        raw = rng.integers(-3000, 3000, nbuf * w.samples_per_buffer, dtype=np.int16)
+        infile = tmp_path / f"in{nbuf}.s16"
+        raw.tofile(infile)
+        t0 = time.perf_counter()
+        with open(infile, "rb") as fin:
+            r = subprocess.run(args, stdin=fin, stdout=subprocess.PIPE, stderr=subprocess.PIPE, env=env, timeout=600)
+        times[nbuf] = time.perf_counter() - t0
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        n_spec = nbuf * w.ffts_per_buf // w.averages
+        assert len(r.stdout) == n_spec * (24 + w.fft_size // 2 + 1)
+    per_buf = (times[20] - times[4]) / 16
+    print(f"host binary, C3: {w.samples_per_buffer / per_buf / 1e6:.1f} Msamples/s "
+          f"({per_buf * 1e3:.2f} ms per buffer of {w.samples_per_buffer} samples)")
