@@ -839,10 +839,24 @@ int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_o
   if (n_spec_expected > 0 && !spec_out) return fail(SK_ERR_ARG, "spectrum records complete in this call but spec_out is null");
   int rc = sk_process_device(pl, pl->d_raw, pl->d_out_ptrs.data(), pl->d_spec, &r, st);
   if (rc) return rc;
-  for (size_t c = 0; c < pl->ch.size(); ++c) {
-    const size_t bytes = sizeof(float2) * (size_t)pl->B * (pl->ch[c].n / 8 * 6);
-    if (bytes == 0) continue;
-    SK_CUDA(cudaMemcpyAsync(chan_out[c], pl->d_out + pl->ch[c].out_off, bytes, cudaMemcpyDeviceToHost, st));
+  // Host outputs laid out like the plan's own buffer (one block, channels in
+  // order) come back in one copy; otherwise one copy per channel.
+  const uint8_t* base = nullptr;
+  bool contiguous = pl->out_total > 0;
+  for (size_t c = 0; c < pl->ch.size() && contiguous; ++c) {
+    if (pl->ch[c].n < 8) continue;
+    const uint8_t* want = base ? base + sizeof(float2) * pl->ch[c].out_off : nullptr;
+    if (!base) base = (const uint8_t*)chan_out[c] - sizeof(float2) * pl->ch[c].out_off;
+    else if ((const uint8_t*)chan_out[c] != want) contiguous = false;
+  }
+  if (contiguous && base) {
+    SK_CUDA(cudaMemcpyAsync((void*)base, pl->d_out, sizeof(float2) * pl->out_total, cudaMemcpyDeviceToHost, st));
+  } else {
+    for (size_t c = 0; c < pl->ch.size(); ++c) {
+      const size_t bytes = sizeof(float2) * (size_t)pl->B * (pl->ch[c].n / 8 * 6);
+      if (bytes == 0) continue;
+      SK_CUDA(cudaMemcpyAsync(chan_out[c], pl->d_out + pl->ch[c].out_off, bytes, cudaMemcpyDeviceToHost, st));
+    }
   }
   if (r.n_spectra)
     SK_CUDA(cudaMemcpyAsync(spec_out, pl->d_spec, (size_t)r.n_spectra * pl->K * pl->spec_bin_bytes, cudaMemcpyDeviceToHost, st));

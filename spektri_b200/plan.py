@@ -146,9 +146,14 @@ class Plan:
 
     # ----------------------------------------------------------- processing
     def empty_outputs(self, pinned: bool = False):
-        """Host buffers for one call: (channel outputs, spectrum buffer)."""
+        """Host buffers for one call: (channel outputs, spectrum buffer).  The
+        channel outputs are views of one block in channel order, which the
+        host path fills with a single copy."""
         mk = pinned_empty if pinned else (lambda s, d: np.empty(s, d))
-        outs = [mk((c["out_samples"],), np.complex64) for c in self.channels]
+        sizes = [c["out_samples"] for c in self.channels]
+        block = mk((max(1, sum(sizes)),), np.complex64)
+        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
+        outs = [block[offs[i]:offs[i + 1]] for i in range(len(sizes))]
         spec = mk((self.max_spectra * self.spectrum_bytes,), np.uint8)
         return outs, spec
 

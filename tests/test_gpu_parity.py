@@ -406,3 +406,20 @@ def test_chirp_limits():
         plan.set_tuning(4096, 256, 1)
     plan.set_tuning(8192, 256, 1)
     assert plan.autotune("")[0] == 8192                          # no cache file
+
+
+def test_host_outputs_contiguous_and_separate():
+    """The host path fills outputs laid out as one block with a single copy and
+    separately allocated outputs with one copy each; both give the same bytes."""
+    w = workloads.c1()
+    raw = workloads.stream_numpy(w, 0, 2 * w.samples_per_buffer).view(np.uint8)
+    r0, r1 = np.split(raw, 2)
+    pa = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 8)
+    pb = make_plan(w.fs, w.fft_size, w.fmt, w.filters(), w.ffts_per_buf, 8)
+    for r in (r0, r1):
+        _, oa = pa.process(r)                                          # one block
+        ob = [np.ascontiguousarray(np.full(c["out_samples"], np.nan, np.complex64)) for c in pb.channels]
+        spec = np.empty(pb.max_spectra * pb.spectrum_bytes, np.uint8)
+        pb.process_into(r, ob, spec)
+        for a, b in zip(oa, ob):
+            assert np.array_equal(a, b)
