@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
   for (int b0 = 0; b0 < a.B; b0 += WELCH_CHUNK) {
     const int nb = min(WELCH_CHUNK, a.B - b0);
     // Phase A: warp w forms blocks w, w + WARPS, ... (independent loads).
-#pragma unroll 2
+#pragma unroll 4
     for (int i = wid; i < nb; i += WELCH_WARPS) {
       const float2* Zb = s.Z + ((size_t)(b0 + i) << s.log2Nc);
       const float2 x1 = x_at<REAL>(s, Zb, kk);

@@ -15,7 +15,7 @@ constexpr int MAX_TILE_TRANSFORMS = 256;  // transforms per filter-bank tile
 // Tile in shared memory: S complex values with one pad slot per 16.
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
 constexpr int WELCH_WARP_BINS = 30;       // bins per Welch CTA (a warp plus a 1-bin halo each side)
-constexpr int WELCH_WARPS = 8;            // warps per Welch CTA (they split the blocks)
+constexpr int WELCH_WARPS = 4;            // warps per Welch CTA (they split the blocks; 4 measured best of 1..32)
 constexpr int WELCH_CHUNK = 64;           // blocks whose Welch terms a CTA stages at once
 
 struct ChanDev {               // one filter-bank channel, as the kernels see it
