@@ -11,7 +11,7 @@ namespace sk {
 constexpr int TILE_S = 8192;              // complex elements per FFT tile
 constexpr int TILE_T = 256;               // threads per tile CTA (32 elements each)
 constexpr int TILE_LOGS = 13;
-constexpr int MAX_TILE_TRANSFORMS = 256;  // transforms per filter-bank tile
+constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
 // Tile in shared memory: S complex values with one pad slot per 16.
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
 constexpr int WELCH_WARP_BINS = 30;       // bins per Welch CTA (a warp plus a 1-bin halo each side)
