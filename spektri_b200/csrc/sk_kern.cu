@@ -47,7 +47,10 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
   return cudaGetLastError();
 }
 
-const void* welch_kernel_ptr(bool cplx) {
+// Up to WELCH_BINS_MAX_B blocks per buffer each warp walks its own bins over
+// all blocks; above that the warps of a CTA split the blocks.
+const void* welch_kernel_ptr(bool cplx, int B) {
+  if (B <= WELCH_BINS_MAX_B) return cplx ? (const void*)welch_bins_kernel<false> : (const void*)welch_bins_kernel<true>;
   return cplx ? (const void*)welch_kernel<false> : (const void*)welch_kernel<true>;
 }
 
@@ -59,6 +62,13 @@ cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) 
 }
 
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
+  if (w.B <= WELCH_BINS_MAX_B) {
+    constexpr int bins_per_cta = WELCH_WARP_BINS * WELCH_WARPS;
+    const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
+    if (cplx) welch_bins_kernel<false><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
+    else welch_bins_kernel<true><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
+    return cudaGetLastError();
+  }
   constexpr int bins_per_cta = WELCH_WARP_BINS;
   const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
   if (cplx) welch_kernel<false><<<g, 32 * WELCH_WARPS, 0, st>>>(w);

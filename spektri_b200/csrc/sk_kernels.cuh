@@ -371,6 +371,42 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
   if (summer) a.acc[kb] = acc;
 }
 
+// The same records for few blocks per buffer: each warp owns its own 30 bins
+// (+ a 1-bin halo each side) and walks every block in order, accumulating in
+// registers -- the same additions in the same order as welch_kernel's
+// phase B, with no shared memory and no barrier.
+template <bool REAL>
+__global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs a) {
+  constexpr int CB = WELCH_WARP_BINS;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int k0 = (blockIdx.x * WELCH_WARPS + wid) * CB;
+  if (k0 >= a.s.K) return;                                   // whole warp: no shuffle partner left behind
+  const int kk = k0 - 1 + lane;
+  const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
+  const SplitArgs& s = a.s;
+  float acc = owner ? a.acc[kk] : 0.0f;
+  int cnt = a.accn0, r = 0;
+#pragma unroll 4
+  for (int b = 0; b < a.B; ++b) {
+    const float2* Zb = s.Z + ((size_t)b << s.log2Nc);
+    const float2 x1 = x_at<REAL>(s, Zb, kk);
+    const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
+    const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
+    if (owner) {
+      s.X[(size_t)b * s.K + kk] = x1;
+      const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
+      acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
+    }
+    if (++cnt >= a.averages) {
+      if (owner) emit_record(a, r, kk, acc, cnt);
+      acc = 0.0f;
+      cnt = 0;
+      ++r;
+    }
+  }
+  if (owner) a.acc[kk] = acc;
+}
+
 // ----------------------------------------------------------------- filter bank
 // CHIRP: the chirp-z tiles of the list (their own launch); else the
 // power-of-two tiles.

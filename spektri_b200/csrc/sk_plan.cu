@@ -418,7 +418,7 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     std::vector<cudaGraphNode_t> nodes(n);
     cudaGraphGetNodes(g, nodes.data(), &n);
     const void* f_fwd = fwd_kernel_ptr(pl->fmt, fwd_kind(pl));
-    const void* f_welch = welch_kernel_ptr(pl->cplx);
+    const void* f_welch = welch_kernel_ptr(pl->cplx, pl->B);
     for (auto nd : nodes) {
       cudaGraphNodeType t;
       if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;

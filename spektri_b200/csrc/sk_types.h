@@ -16,6 +16,7 @@ constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
 constexpr int WELCH_WARP_BINS = 30;       // bins per Welch CTA (a warp plus a 1-bin halo each side)
 constexpr int WELCH_WARPS = 4;            // warps per Welch CTA (they split the blocks; 4 measured best of 1..32)
+constexpr int WELCH_BINS_MAX_B = 16;      // blocks per buffer up to which a warp walks its own bins
 constexpr int WELCH_CHUNK = 64;           // blocks whose Welch terms a CTA stages at once
 
 struct ChanDev {               // one filter-bank channel, as the kernels see it
@@ -146,6 +147,6 @@ const void* fwd_kernel_ptr(int fmt, int kind);
 const void* fwd_kernel_ptr_8(int fmt, int kind);
 const void* fwd_kernel_ptr_16(int fmt, int kind);
 const void* fwd_kernel_ptr_32(int fmt, int kind);
-const void* welch_kernel_ptr(bool cplx);
+const void* welch_kernel_ptr(bool cplx, int B);
 
 }  // namespace sk
