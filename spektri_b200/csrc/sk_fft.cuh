@@ -96,11 +96,24 @@ struct TileShape {
   static constexpr size_t SMEM_BYTES = sizeof(float2) * (size_t)SMEM_ELEMS;
 };
 
+// Shared-memory index policies: padx, and padx plus one slot per transform
+// (for tiles written column-wise, one transform per column: with 2^logn-point
+// transforms the column stride n + n/16 + 1 is odd in 8-byte slots for
+// n >= 32, so a warp writing 32 consecutive columns hits every bank pair).
+struct PadX {
+  __device__ __forceinline__ int operator()(int e) const { return padx(e); }
+};
+struct PadCols {
+  int logn;
+  __device__ __forceinline__ int operator()(int e) const { return padx(e) + (e >> logn); }
+};
+
 // One Stockham stage of radix R over the whole tile (S/n transforms).
 // Reads, sync, writes, sync: the caller syncs before the first stage.
 // tw: forward table W_S^k, k in [0, S).
-template <int R, int DIR, int S, int T>
-__device__ __forceinline__ void tile_stage(float2* sm, const float2* __restrict__ tw, int log2n, int log2L) {
+template <int R, int DIR, int S, int T, class Pad = PadX>
+__device__ __forceinline__ void tile_stage(float2* sm, const float2* __restrict__ tw, int log2n, int log2L,
+                                           const Pad& pad = Pad()) {
   constexpr int NB = S / (R * T);
   static_assert(NB >= 1, "radix larger than elements per thread");
   constexpr int LOGR = ilog2c(R);
@@ -117,7 +130,7 @@ __device__ __forceinline__ void tile_stage(float2* sm, const float2* __restrict_
     const int g = q >> log2L;
     const int base = t << log2n;
 #pragma unroll
-    for (int s = 0; s < R; ++s) v[bb][s] = sm[padx(base + q + (s << log2nR))];
+    for (int s = 0; s < R; ++s) v[bb][s] = sm[pad(base + q + (s << log2nR))];
     if (log2L > 0) {
       const int sh = LOGS - log2L - LOGR;       // S / (L R) = 2^sh
 #pragma unroll
@@ -134,7 +147,7 @@ __device__ __forceinline__ void tile_stage(float2* sm, const float2* __restrict_
 #pragma unroll
   for (int bb = 0; bb < NB; ++bb) {
 #pragma unroll
-    for (int u = 0; u < R; ++u) sm[padx(ob[bb] + (u << log2L))] = v[bb][u];
+    for (int u = 0; u < R; ++u) sm[pad(ob[bb] + (u << log2L))] = v[bb][u];
   }
   __syncthreads();
 }
@@ -161,18 +174,18 @@ __device__ __forceinline__ int stage_radix(int log2n, int p) {
 }
 
 // All stages of a batched 2^log2n-point FFT over the tile in shared memory.
-template <int DIR, int S, int T>
-__device__ __forceinline__ void tile_fft(float2* sm, const float2* __restrict__ tw, int log2n) {
+template <int DIR, int S, int T, class Pad = PadX>
+__device__ __forceinline__ void tile_fft(float2* sm, const float2* __restrict__ tw, int log2n, const Pad& pad = Pad()) {
   int log2L = 0;
 #pragma unroll 1
   for (int p = 0; p < 3; ++p) {
     const int lr = stage_radix(log2n, p);
     if (lr == 0) break;
     switch (lr) {
-      case 2: tile_stage<4, DIR, S, T>(sm, tw, log2n, log2L); break;
-      case 3: tile_stage<8, DIR, S, T>(sm, tw, log2n, log2L); break;
-      case 4: tile_stage<16, DIR, S, T>(sm, tw, log2n, log2L); break;
-      case 5: tile_stage<32, DIR, S, T>(sm, tw, log2n, log2L); break;
+      case 2: tile_stage<4, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
+      case 3: tile_stage<8, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
+      case 4: tile_stage<16, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
+      case 5: tile_stage<32, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
     }
     log2L += lr;
   }

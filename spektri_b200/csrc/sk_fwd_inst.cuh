@@ -21,7 +21,7 @@ cudaError_t fwd_col_launch_one(int grid, const FwdArgs& a, float2* Y, cudaStream
     const long long cols = (long long)a.B << TILE_LOGS;
     fwd_colreg_kernel<FMT><<<(unsigned)((cols + 255) / 256), 256, 0, st>>>(a, Y);
   } else {
-    fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
+    fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM_COL, st>>>(a, Y);
   }
   return cudaGetLastError();
 }
@@ -32,7 +32,7 @@ cudaError_t fwd_prepare_one() {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(fwd_col_kernel<TILE_S, TILE_T, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)TILE_SMEM);
+                              (int)TILE_SMEM_COL);
 }
 
 // kind 0: single-pass kernel; 1: shared-memory column pass; 2: register column pass.

@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
       a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
   }
   const int LOGR1 = a.log2R1, R1 = 1 << LOGR1, LOGC = LOGS - LOGR1, C = 1 << LOGC;
+  const PadCols pad{LOGR1};                                 // consecutive threads write consecutive columns
   const int b = blockIdx.x >> LOGR1;
   const int c0 = (blockIdx.x & (R1 - 1)) << LOGC;
   const long long p0 = (long long)b * a.hop;
@@ -178,17 +179,17 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
     const int j1 = g >> LOGC, col = g & (C - 1);
     const int jj = (j1 << LOGS) + c0 + col;
     const float2 z = src.pair(p0 + (CPLX ? jj : 2 * jj));
-    sm[padx((col << LOGR1) + j1)] = make_float2(z.x * a.wscale, z.y * a.wscale);
+    sm[pad((col << LOGR1) + j1)] = make_float2(z.x * a.wscale, z.y * a.wscale);
   }
   __syncthreads();
-  tile_fft<-1, S, T>(sm, a.tw_tile, LOGR1);
+  tile_fft<-1, S, T>(sm, a.tw_tile, LOGR1, pad);
   const int shC = a.log2N - a.log2Nc;
   float2* Yb = Y + ((size_t)b << a.log2Nc);
 #pragma unroll 4
   for (int k = 0; k < E; ++k) {
     const int g = threadIdx.x + k * T;
     const int k1 = g >> LOGC, col = g & (C - 1);
-    float2 v = sm[padx((col << LOGR1) + k1)];
+    float2 v = sm[pad((col << LOGR1) + k1)];
     if (k1) v = cmul(v, __ldg(&a.tw_big[((c0 + col) * k1) << shC]));
     Yb[((size_t)k1 << LOGS) + c0 + col] = v;
   }

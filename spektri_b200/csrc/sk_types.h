@@ -14,6 +14,8 @@ constexpr int TILE_LOGS = 13;
 constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
 // Tile in shared memory: S complex values with one pad slot per 16.
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
+// The column pass's tile adds one slot per transform (at most S/16 of them).
+constexpr size_t TILE_SMEM_COL = sizeof(float2) * (size_t)(TILE_S + TILE_S / 8);
 constexpr int WELCH_WARP_BINS = 30;       // bins per Welch CTA (a warp plus a 1-bin halo each side)
 constexpr int WELCH_WARPS = 4;            // warps per Welch CTA (they split the blocks; 4 measured best of 1..32)
 constexpr int WELCH_BINS_MAX_B = 16;      // blocks per buffer up to which a warp walks its own bins
