@@ -117,8 +117,9 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
 
 // Stages 2..: span L = 2^LOGL (LOGL = 0: a first stage run from shared
 // memory, in place).  LAST: q < L, g = 0, output o = q + u L.
-template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store>
-__device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store) {
+template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store, class Pad = PadX>
+__device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store,
+                                           const Pad& pad = Pad()) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   constexpr int SH = TILE_LOGS - LOGL - LOGR;            // tw is the 2^13-point table
   static_assert(NB >= 1 && SH >= 0, "bad stage");
@@ -133,7 +134,7 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
       const int base = t << LOGN;
       float2 v[R];
 #pragma unroll
-      for (int s = 0; s < R; ++s) v[s] = sm[padx(base + q + (s << LOGNR))];
+      for (int s = 0; s < R; ++s) v[s] = sm[pad(base + q + (s << LOGNR))];
       twiddle(v, q);
       dft<R, DIR>(v);
       if (t < count) {
@@ -149,7 +150,7 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
       const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
       const int base = t << LOGN;
 #pragma unroll
-      for (int s = 0; s < R; ++s) v[bb][s] = sm[padx(base + q + (s << LOGNR))];
+      for (int s = 0; s < R; ++s) v[bb][s] = sm[pad(base + q + (s << LOGNR))];
       twiddle(v[bb], q & ((1 << LOGL) - 1));
       dft<R, DIR>(v[bb]);
     }
@@ -161,7 +162,7 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
       const int j = q & ((1 << LOGL) - 1), g = q >> LOGL;
       const int ob = (t << LOGN) + (g << (LOGL + LOGR)) + j;
 #pragma unroll
-      for (int u = 0; u < R; ++u) sm[padx(ob + (u << LOGL))] = v[bb][u];
+      for (int u = 0; u < R; ++u) sm[pad(ob + (u << LOGL))] = v[bb][u];
     }
   }
 }
@@ -242,6 +243,29 @@ __device__ __forceinline__ void tile_chirp(float2* sm, int count, const float2* 
       __syncthreads();
       stage_next<LOGM, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, +1, true>(sm, count, tw, store);
     }
+  }
+}
+
+// Every 2^LOGN-point transform of the tile, already in shared memory (index
+// policy pad), transformed in place: each stage reads all its inputs, syncs,
+// writes; the caller syncs before and after.
+template <int LOGN, int S, int T, int DIR, class Pad>
+__device__ __forceinline__ void tile_fft_inplace(float2* sm, const float2* __restrict__ tw, const Pad& pad) {
+  using P = StagePlan<LOGN, S / T>;
+  constexpr int count = S >> LOGN;
+  auto none = [](int, int, float2) {};
+  stage_next<LOGN, 1 << P::r0, 0, S, T, DIR, false>(sm, count, tw, none, pad);
+  if constexpr (P::ns >= 2) {
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, none, pad);
+  }
+  if constexpr (P::ns >= 3) {
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, none, pad);
+  }
+  if constexpr (P::ns >= 4) {
+    __syncthreads();
+    stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, false>(sm, count, tw, none, pad);
   }
 }
 

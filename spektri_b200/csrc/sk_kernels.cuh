@@ -182,7 +182,14 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
     sm[pad((col << LOGR1) + j1)] = make_float2(z.x * a.wscale, z.y * a.wscale);
   }
   __syncthreads();
-  tile_fft<-1, S, T>(sm, a.tw_tile, LOGR1, pad);
+  switch (LOGR1) {                                          // R1-point column transforms, in place
+    case 4: tile_fft_inplace<4, S, T, -1>(sm, a.tw_tile, pad); break;
+    case 5: tile_fft_inplace<5, S, T, -1>(sm, a.tw_tile, pad); break;
+    case 6: tile_fft_inplace<6, S, T, -1>(sm, a.tw_tile, pad); break;
+    case 7: tile_fft_inplace<7, S, T, -1>(sm, a.tw_tile, pad); break;
+    case 8: tile_fft_inplace<8, S, T, -1>(sm, a.tw_tile, pad); break;
+  }
+  __syncthreads();
   const int shC = a.log2N - a.log2Nc;
   float2* Yb = Y + ((size_t)b << a.log2Nc);
 #pragma unroll 4
