@@ -69,7 +69,7 @@ struct SampleSrc {
 template <int LOGN, int S, int T, int FMT>
 __device__ __forceinline__ void fwd_tile_blocks(float2* sm, const FwdArgs& a, const SampleSrc<FMT>& src, int tile) {
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
-  constexpr int per = S >> LOGN;
+  const int per = a.per > 0 ? a.per : S >> LOGN;
   const int b0 = tile * per;
   const int count = min(per, a.B - b0);
   auto load = [&](int t, int j) {

@@ -60,6 +60,7 @@ struct sk_plan {
   long long N = 0, overlap = 0, hop = 0, nnew = 0, total = 0;
   int K = 0, B = 0;
   int log2N = 0, log2Nc = 0, R1 = 1, log2R1 = 0;
+  int fwd_per = 1;                      // single-pass forward FFT (Nc <= 8192): blocks per tile
   float wscale = 0.f;
   int spec_fmt = 0, spec_bin_bytes = 1;
   int averages = 1;
@@ -218,12 +219,13 @@ FwdArgs fwd_args(const sk_plan* pl, const uint8_t* raw) {
   a.tw_tile = pl->d_tw_tile;
   a.tw_big = pl->d_tw_big;
   a.Z = pl->d_Z;
+  a.per = pl->fwd_per;
   return a;
 }
 
 int fwd_grid(const sk_plan* pl) {
   if (pl->R1 == 1) {
-    const int per = S >> pl->log2Nc;
+    const int per = pl->fwd_per;
     return (pl->B + per - 1) / per;
   }
   return pl->B * pl->R1;
@@ -641,8 +643,16 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
 
   // Work lists, one per tile size.  Batched: channels grouped by IFFT size,
   // largest first, each size's (channel, block) transforms packed size/n to a
-  // tile (an n = 2 size transform takes two tiles, one per output parity).
-  // Plain: each channel's own tiles.
+  // tile (an n = 2 size transform takes two tiles, one per output parity);
+  // when that leaves fewer tiles than SMs, fewer transforms go to a tile
+  // (halving until there are enough, or one per tile), so small buffers still
+  // spread over the GPU.  Plain: each channel's own tiles.
+  int n_sm = 1;
+  CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, p.device));
+  if (pl->R1 == 1) {                    // the single-pass forward FFT: the same rule for its tiles of blocks
+    pl->fwd_per = S >> pl->log2Nc;
+    while (pl->fwd_per > 1 && (pl->B + pl->fwd_per - 1) / pl->fwd_per < n_sm) pl->fwd_per >>= 1;
+  }
   for (int k = 0; k < 2; ++k) {
     sk_plan::TileSet& t = pl->ts[k];
     t.size = k == 0 ? TILE_S : TILE_S / 2;
@@ -659,6 +669,31 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
         }
     };
     auto per_tile = [&](int l2) { return l2 > logt ? 1 : std::min(t.size >> l2, MAX_TILE_TRANSFORMS); };
+    int shrink = 0;                     // batched tiles hold per >> shrink transforms (at least 1)
+    {
+      std::vector<std::pair<long long, int>> groups;   // (transforms, full per-tile count)
+      for (const auto& d : pl->h_blu)
+        if (d.logm <= logt) {
+          long long cnt = 0;
+          for (const auto& c : pl->ch) cnt += (c.log2n == 0 && c.n == (uint32_t)d.n) ? pl->B : 0;
+          groups.push_back({cnt, std::min(t.size >> d.logm, MAX_TILE_TRANSFORMS)});
+        }
+      for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
+        long long cnt = 0;
+        for (const auto& c : pl->ch) cnt += c.log2n == l2 ? (long long)pl->B * (l2 > logt ? 2 : 1) : 0;
+        if (cnt) groups.push_back({cnt, per_tile(l2)});
+      }
+      for (;; ++shrink) {
+        long long ntiles = 0;
+        bool all_one = true;
+        for (const auto& g : groups) {
+          const long long per = std::max(1, g.second >> shrink);
+          ntiles += (g.first + per - 1) / per;
+          all_one = all_one && per == 1;
+        }
+        if (all_one || ntiles >= n_sm) break;
+      }
+    }
     // chirp-z sizes first (the most work per point), largest transform first
     for (int lm = TILE_LOGS; lm >= 4; --lm)
       for (size_t k = 0; k < pl->h_blu.size(); ++k) {
@@ -667,7 +702,8 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
         const int base = (int)list.size();
         for (size_t c = 0; c < pl->ch.size(); ++c)
           if (pl->ch[c].blu == (int)k) add((int)c, 0);
-        const int cnt = (int)list.size() - base, per = std::min(t.size >> lm, MAX_TILE_TRANSFORMS);
+        const int cnt = (int)list.size() - base;
+        const int per = std::max(1, std::min(t.size >> lm, MAX_TILE_TRANSFORMS) >> shrink);
         for (int o = 0; o < cnt; o += per)
           tiles.push_back(TileDesc{BLU_TAG + lm, base + o, std::min(per, cnt - o), (int)k});
       }
@@ -676,7 +712,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       const int base = (int)list.size();
       for (size_t c = 0; c < pl->ch.size(); ++c)
         if (pl->ch[c].log2n == l2) add((int)c, l2);
-      const int cnt = (int)list.size() - base, per = per_tile(l2);
+      const int cnt = (int)list.size() - base, per = std::max(1, per_tile(l2) >> shrink);
       for (int o = 0; o < cnt; o += per) tiles.push_back(TileDesc{l2, base + o, std::min(per, cnt - o), 0});
     }
     t.n_batched = (int)tiles.size();

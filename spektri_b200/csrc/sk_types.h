@@ -66,6 +66,7 @@ struct FwdArgs {
   const float2* tw_tile;       // W_S^k
   const float2* tw_big;        // W_N^k, k < N
   float2* Z;                   // [B][Nc]; for R1 > 1 element k1 + R1*k2 sits at k1*S + k2
+  int per;                     // Nc <= S: blocks per tile (0: S / Nc, a full tile)
 };
 
 struct SplitArgs {
