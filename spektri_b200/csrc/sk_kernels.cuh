@@ -2,15 +2,18 @@
 //
 // Per input buffer of B overlapped blocks (block b = samples [b*hop, b*hop+N)
 // of [N/4 carried samples | 3N/4*B new samples], main.rs:162-181, dsp.rs:150-155):
-//   fwd_fft_kernel      raw samples -> converted, scaled by scaling/N, forward
-//                       FFT of size Nc (N/2 complex pairs for real input, N for
-//                       complex) -> Z                                       [multifft.rs]
-//   welch_split_kernel  Z -> X (K bins, real-input split), and the Welch term
-//                       |X[k] - (X[k-1]+X[k+1])/2|^2 per block -> P        [spectrum.rs:90-111]
-//   welch_accum_kernel  P -> running f32 accumulator in block order, emits and
-//                       quantises records                                  [spectrum.rs:112-161]
-//   fcfb_kernel         per channel and block: gather n bins (modulo/mirror),
-//                       times weights, inverse FFT, keep [n/8, 7n/8)        [fcfb.rs:154-188]
+//   fwd_fft_kernel       raw samples -> converted, scaled by scaling/N, forward
+//                        FFT of size Nc (N/2 complex pairs for real input, N for
+//                        complex) -> Z, whole blocks per tile (Nc <= 8192)  [multifft.rs]
+//   fwd_colreg_kernel /  two-pass forward FFT for Nc = R1 * 8192: column pass
+//   fwd_col_kernel       (registers for R1 <= 8, shared memory above) -> Y,
+//   + fwd_row_kernel     then 8192-point rows -> Z in residue layout
+//   welch_kernel /       Z -> X (K bins, real-input split), the Welch term
+//   welch_bins_kernel    |X[k] - (X[k-1]+X[k+1])/2|^2, its f32 accumulation in
+//                        block order, emission and quantisation of records [spectrum.rs:82-163]
+//   welch_split_kernel   Z -> X only (the differentiable stage, the allocation-free entry)
+//   fcfb_kernel          per channel and block: gather n bins (modulo/mirror),
+//                        times weights, inverse FFT, keep [n/8, 7n/8)        [fcfb.rs:154-188]
 //   fcfb_backward_kernel adjoint of fcfb_kernel for weight design
 #pragma once
 #include "sk_types.h"
