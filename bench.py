@@ -203,6 +203,8 @@ def main():
     ap.add_argument("--ffts-per-buf", type=int, default=0, help="override blocks per buffer (small profiling cases)")
     ap.add_argument("--preroll", type=float, default=1.5, help="seconds of untimed steps while clocks are sampled")
     ap.add_argument("--tuning", default="", help="SIZE,THREADS,CTAS_PER_SM: fixed filter-bank tile shape instead of autotuning")
+    ap.add_argument("--by-size", action="store_true",
+                    help="also time the filter bank of each IFFT size alone (same tile shape)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_setup()
@@ -342,6 +344,33 @@ def main():
         result["plain_value"] = round(vp, 2)
         result["batched_over_plain"] = round(value / ws / vp, 2)
         del pp
+
+    if args.by_size:
+        # Each IFFT size alone: a plan holding only that size's channels, the
+        # same tile shape, its filter-bank launch timed under CUDA events.
+        # Each figure includes one launch's fixed cost (claims, tail).
+        by = {}
+        for n in sorted({c["n"] for c in w.channels}):
+            fl = [f for f, c in zip(w.filters(), w.channels) if c["n"] == n]
+            ps = Plan(w.fs, w.fft_size, w.fmt, fl, fc_in=w.fc, ffts_per_buf=w.ffts_per_buf,
+                      averages=w.averages, spectrum_format="f32", mode="batched", device=dev)
+            try:
+                ps.set_tuning(tile_size, tile_threads, ctas_per_sm)
+            except Exception:
+                ps.autotune()
+            o2 = [torch.empty(c["out_samples"], dtype=torch.complex64, device=dev) for c in ps.channels]
+            with torch.cuda.stream(st):
+                for i in range(args.warmup):
+                    ps.process_device(raws[i % nbuf], o2, spec, stream=st)
+                ps.set_timing(True)
+                for i in range(min(args.steps, 50)):
+                    ps.process_device(raws[i % nbuf], o2, spec, stream=st)
+            torch.cuda.synchronize(dev)
+            sm_, nc = ps.timing()
+            by[str(n)] = {"channels": len(fl), "points": len(fl) * n * w.ffts_per_buf,
+                          "fcfb_us": round(sm_[2] / max(1, nc) * 1e3, 2)}
+            del ps, o2
+        result["fcfb_by_size"] = by
 
     # End to end through the public host API, with pinned host buffers.
     ke = max(1, min(args.e2e_steps, args.steps))
