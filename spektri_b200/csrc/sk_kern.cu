@@ -42,9 +42,27 @@ cudaError_t launch_fwd_col(int fmt, int grid, const FwdArgs& a, float2* Y, cudaS
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st) {
-  fwd_row_kernel<TILE_S, TILE_T><<<grid, TILE_T, TILE_SMEM, st>>>(a, Y);
-  return cudaGetLastError();
+cudaError_t launch_kernel(const void* fn, dim3 grid, dim3 block, void** params, size_t smem, cudaStream_t st,
+                          bool pdl) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, fn, params);
+}
+
+cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st, bool pdl) {
+  FwdArgs args = a;
+  const float2* y = Y;
+  void* params[] = {(void*)&args, (void*)&y};
+  return launch_kernel((const void*)fwd_row_kernel<TILE_S, TILE_T>, dim3(grid), dim3(TILE_T), params, TILE_SMEM, st,
+                       pdl);
 }
 
 // Up to WELCH_BINS_MAX_B blocks per buffer each warp walks its own bins over
@@ -61,19 +79,12 @@ cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) 
   return cudaGetLastError();
 }
 
-cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st) {
-  if (w.B <= WELCH_BINS_MAX_B) {
-    constexpr int bins_per_cta = WELCH_WARP_BINS * WELCH_WARPS;
-    const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
-    if (cplx) welch_bins_kernel<false><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
-    else welch_bins_kernel<true><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
-    return cudaGetLastError();
-  }
-  constexpr int bins_per_cta = WELCH_WARP_BINS;
+cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl) {
+  const int bins_per_cta = w.B <= WELCH_BINS_MAX_B ? WELCH_WARP_BINS * WELCH_WARPS : WELCH_WARP_BINS;
   const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
-  if (cplx) welch_kernel<false><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
-  else welch_kernel<true><<<g, 32 * WELCH_WARPS, 0, st>>>(w);
-  return cudaGetLastError();
+  WelchArgs args = w;
+  void* params[] = {(void*)&args};
+  return launch_kernel(welch_kernel_ptr(cplx, w.B), dim3(g), dim3(32 * WELCH_WARPS), params, 0, st, pdl);
 }
 
 // Filter-bank tile shapes (tile size x threads, minimum CTAs per SM):
@@ -119,12 +130,12 @@ cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* per_sm) {
 }
 
 cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
-                        const FcfbArgs& a, int tile_base, cudaStream_t st) {
+                        const FcfbArgs& a, int tile_base, cudaStream_t st, bool pdl) {
   FcfbArgs args = a;
   int base = tile_base;
   void* params[] = {(void*)&args, (void*)&base};
-  return cudaLaunchKernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent, chirp), dim3(grid), dim3(tile_threads),
-                          params, fcfb_smem(tile_size), st);
+  return launch_kernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent, chirp), dim3(grid), dim3(tile_threads),
+                       params, fcfb_smem(tile_size), st, pdl);
 }
 
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st) {

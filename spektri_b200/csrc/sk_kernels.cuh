@@ -22,6 +22,26 @@
 
 namespace sk {
 
+// Programmatic dependent launch.  In the batched graph the row pass, the Welch
+// kernel and the filter bank are launched with programmatic stream
+// serialization: their CTAs launch as soon as every CTA of the kernel ahead of
+// them has exited (no early trigger: dependents that became resident early
+// slowed the kernel they waited on), do what does not depend on it (tile
+// claims, metadata) while that kernel's grid completes, and block in
+// pdl_wait() until its writes are visible.  A no-op for a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// The first forward kernel of a batched call zeroes the filter bank's tile
+// cursors (the previous call's filter bank has completed: graph launches are
+// serialised).
+__device__ __forceinline__ void reset_cursors(int* cursor) {
+  if (cursor && blockIdx.x == 0 && threadIdx.x == 0) {
+    cursor[0] = 0;
+    cursor[1] = 0;
+  }
+}
+
 // ----------------------------------------------------------------- input formats
 // One scalar component of a raw sample (inputformats.rs:65-155).  BASE is the
 // format code without its complex bit.
@@ -118,6 +138,7 @@ template <int S, int T, int FMT>
 __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry: convert the last N/4 new samples for the next buffer (main.rs:173)
     const long long stride = (long long)gridDim.x * T;
@@ -163,6 +184,7 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
   constexpr int E = S / T, LOGS = ilog2c(S);
+  reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry, as in fwd_fft_kernel
     const long long stride = (long long)gridDim.x * T;
@@ -233,6 +255,7 @@ __device__ __forceinline__ void fwd_cols_reg(const FwdArgs& a, const SampleSrc<F
 template <int FMT>
 __global__ void __launch_bounds__(256) fwd_colreg_kernel(FwdArgs a, float2* Y) {
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry, as in fwd_fft_kernel
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -254,6 +277,7 @@ template <int S, int T>
 __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* Y) {
   extern __shared__ float2 sm[];
   constexpr int LOGS = ilog2c(S);
+  pdl_wait();                                               // Y from the column pass
   const int b = blockIdx.x >> a.log2R1, k1 = blockIdx.x & (a.R1 - 1);
   const size_t off = ((size_t)b << a.log2Nc) + ((size_t)k1 << LOGS);
   const float2* Yr = Y + off;
@@ -339,6 +363,7 @@ template <bool REAL>
 __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
   constexpr int CB = WELCH_WARP_BINS;                        // bins per CTA (every warp covers them)
   __shared__ float terms[WELCH_CHUNK][CB];
+  pdl_wait();                                               // Z from the forward FFT
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k0 = blockIdx.x * CB;
   const int kk = k0 - 1 + lane;                              // bin this lane forms
@@ -389,6 +414,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
 template <bool REAL>
 __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs a) {
   constexpr int CB = WELCH_WARP_BINS;
+  pdl_wait();                                               // Z from the forward FFT
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k0 = (blockIdx.x * WELCH_WARPS + wid) * CB;
   if (k0 >= a.s.K) return;                                   // whole warp: no shuffle partner left behind
@@ -461,6 +487,7 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       s_meta[threadIdx.x] = m;
     }
     __syncthreads();
+    if (it == 0) pdl_wait();                                  // X from the Welch kernel
     fcfb_tile_dispatch<S, T, REAL, CHIRP>(td.log2n, sm, s_meta, td.count, c, CHIRP ? a.blu + td.pad : nullptr);
     if constexpr (PERSIST) {
       if (threadIdx.x == 0) s_tile[(it + 1) & 1] = next;

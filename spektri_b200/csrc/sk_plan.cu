@@ -264,11 +264,13 @@ WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
 // above) followed by the row pass into d_Z.
 int fwd_kind(const sk_plan* pl) { return pl->R1 == 1 ? 0 : pl->R1 > 8 ? 1 : 2; }
 
-cudaError_t launch_fwd_any(const sk_plan* pl, const FwdArgs& a, cudaStream_t st) {
+// pdl: the row pass (if any) is launched as a programmatic dependent of the
+// column pass.
+cudaError_t launch_fwd_any(const sk_plan* pl, const FwdArgs& a, cudaStream_t st, bool pdl = false) {
   if (pl->R1 == 1) return launch_fwd(pl->fmt, fwd_grid(pl), a, st);
   const cudaError_t e = launch_fwd_col(pl->fmt, fwd_grid(pl), a, pl->d_Y, st);
   if (e != cudaSuccess) return e;
-  return launch_fwd_rows(fwd_grid(pl), a, pl->d_Y, st);
+  return launch_fwd_rows(fwd_grid(pl), a, pl->d_Y, st, pdl);
 }
 
 int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
@@ -358,35 +360,42 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
 }
 
 // Batched: the chirp-z tiles (if any) in one persistent launch, then the
-// power-of-two tiles in another, each with its own cursor.
-cudaError_t launch_batched(sk_plan* pl, const FcfbArgs& a0, int size, int threads, int grid, cudaStream_t st) {
+// power-of-two tiles in another, each with its own cursor.  graph: the
+// cursors were zeroed by the forward kernel and the first launch is a
+// programmatic dependent of the Welch kernel; otherwise a memset zeroes them.
+cudaError_t launch_batched(sk_plan* pl, const FcfbArgs& a0, int size, int threads, int grid, cudaStream_t st,
+                           bool graph = false) {
   const sk_plan::TileSet& t = pl->ts[size == TILE_S ? 0 : 1];
-  cudaError_t e = cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(int), st);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (!graph) {
+    e = cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+  }
   FcfbArgs a = a0;
   a.tiles = t.d_tiles;
   a.list = t.d_list;
   if (t.n_chirp > 0) {
     a.cursor = pl->d_cursor + 1;
     a.ntiles = t.n_chirp;
-    e = launch_fcfb(pl->cplx, true, true, size, threads, std::min(grid, t.n_chirp), a, 0, st);
+    e = launch_fcfb(pl->cplx, true, true, size, threads, std::min(grid, t.n_chirp), a, 0, st, graph);
     if (e != cudaSuccess) return e;
   }
   if (t.n_batched > t.n_chirp) {
     a.cursor = pl->d_cursor;
     a.tiles = t.d_tiles + t.n_chirp;
     a.ntiles = t.n_batched - t.n_chirp;
-    e = launch_fcfb(pl->cplx, true, false, size, threads, std::min(grid, a.ntiles), a, 0, st);
+    e = launch_fcfb(pl->cplx, true, false, size, threads, std::min(grid, a.ntiles), a, 0, st,
+                    graph && t.n_chirp == 0);
   }
   return e;
 }
 
-int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st) {
+int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st, bool graph = false) {
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, chans, X);
   const sk_plan::TileSet& t = cur_tiles(pl);
   if (batched) {
-    SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st));
+    SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st, graph));
   } else {
     for (size_t c = 0; c < pl->ch.size(); ++c)
       SK_CUDA(launch_fcfb(pl->cplx, false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
@@ -395,19 +404,22 @@ int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, c
   return SK_OK;
 }
 
-// Batched call through the plan's CUDA graph: [forward FFT] -> [split +
-// Welch] -> [cursor reset] -> [persistent filter bank].  The first call
-// captures it on the plan's stream; later calls patch the two kernel nodes
-// whose arguments change (input pointer and carry buffers; Welch state and
-// record buffer) and replay it on `st`.
+// Batched call through the plan's CUDA graph: [forward FFT, which also zeroes
+// the tile cursors] -> [split + Welch] -> [persistent filter bank], each
+// kernel after the first a programmatic dependent of the one before it (its
+// CTAs launch as that one's CTAs exit and wait for its writes on the device).
+// The first call captures it on the plan's stream; later calls patch the two
+// kernel nodes whose arguments change (input pointer and carry buffers; Welch
+// state and record buffer) and replay it on `st`.
 int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t st) {
-  const FwdArgs fa = fwd_args(pl, raw);
+  FwdArgs fa = fwd_args(pl, raw);
+  fa.cursor = pl->d_cursor;
   const WelchArgs wa = welch_args(pl, pl->d_X, wc);
   if (!pl->graph_exec) {
     SK_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t e1 = launch_fwd_any(pl, fa, pl->stream);
-    const cudaError_t e2 = launch_welch(pl->cplx, wa, pl->stream);
-    const int rc = run_fcfb(pl, pl->d_chans, pl->d_X, true, pl->stream);
+    const cudaError_t e1 = launch_fwd_any(pl, fa, pl->stream, true);
+    const cudaError_t e2 = launch_welch(pl->cplx, wa, pl->stream, true);
+    const int rc = run_fcfb(pl, pl->d_chans, pl->d_X, true, pl->stream, true);
     cudaGraph_t g = nullptr;
     const cudaError_t e3 = cudaStreamEndCapture(pl->stream, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || rc != SK_OK || e3 != cudaSuccess) {

@@ -67,6 +67,8 @@ struct FwdArgs {
   const float2* tw_big;        // W_N^k, k < N
   float2* Z;                   // [B][Nc]; for R1 > 1 element k1 + R1*k2 sits at k1*S + k2
   int per;                     // Nc <= S: blocks per tile (0: S / Nc, a full tile)
+  int* cursor;                 // non-null: the filter bank's two tile cursors, zeroed by the
+                               // first forward kernel (the batched graph, in place of a memset)
 };
 
 struct SplitArgs {
@@ -122,9 +124,14 @@ cudaError_t launch_fwd_col(int fmt, int grid, const FwdArgs& a, float2* Y, cudaS
 cudaError_t launch_fwd_col_8(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
 cudaError_t launch_fwd_col_16(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
 cudaError_t launch_fwd_col_32(int fmt, int grid, const FwdArgs& a, float2* Y, cudaStream_t st);
-cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st);
+// pdl: launched with programmatic stream serialization (the kernel's CTAs may
+// start as those of the kernel ahead of it in the stream exit, before that
+// grid has completed; it waits for that grid in pdl_wait()).
+cudaError_t launch_kernel(const void* fn, dim3 grid, dim3 block, void** params, size_t smem, cudaStream_t st,
+                          bool pdl);
+cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st, bool pdl = false);
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
-cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st);
+cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl = false);
 cudaError_t fcfb_prepare();
 // Filter-bank tile shapes (tile_size, tile_threads): (8192, 256), (8192, 512)
 // and (4096, 256); a 4096-point tile runs an 8192-point transform as two halves.
@@ -133,7 +140,7 @@ constexpr size_t fcfb_smem(int tile_size) { return sizeof(float2) * (size_t)(til
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* ctas_per_sm);
 // chirp: the kernel for chirp-z tiles (else power-of-two tiles).
 cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
-                        const FcfbArgs& a, int tile_base, cudaStream_t st);
+                        const FcfbArgs& a, int tile_base, cudaStream_t st, bool pdl = false);
 const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp);
 // Per-shape instance tables (sk_fcfb_*.cu).
 const void* fcfb_ptr_8192(bool cplx, bool persistent);
