@@ -51,6 +51,29 @@ __device__ __forceinline__ float2 twmul32(float2 v, int m) {
   return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
 }
 
+// Radix-2 butterfly (e + W_32^m o, e - W_32^m o) for a compile-time m, with
+// the twiddle folded into fused multiply-adds: 6 instructions instead of 8
+// where W_32^m is not a multiple of i.  For |cos| = |sin| (m = 4, 12, 20, 28)
+// both outputs are c (o.x -/+ o.y, ...) + e and -c (...) + e; otherwise
+// u = e + W o is two FMAs per component and e - W o = 2e - u.
+template <int DIR>
+__device__ __forceinline__ void bfly32(float2 e, float2 o, int m, float2& u, float2& v) {
+  if ((m & 7) == 0) {
+    const float2 t = twmul32<DIR>(o, m);
+    u = cadd(e, t);
+    v = csub(e, t);
+  } else if ((m & 3) == 0) {
+    const float c = cos32(m), r = DIR * sin32(m) / cos32(m);   // r = +-1, exact
+    const float dx = o.x - r * o.y, dy = r * o.x + o.y;
+    u = make_float2(__fmaf_rn(c, dx, e.x), __fmaf_rn(c, dy, e.y));
+    v = make_float2(__fmaf_rn(-c, dx, e.x), __fmaf_rn(-c, dy, e.y));
+  } else {
+    const float c = cos32(m), s = DIR * sin32(m);
+    u = make_float2(__fmaf_rn(o.x, c, __fmaf_rn(-o.y, s, e.x)), __fmaf_rn(o.x, s, __fmaf_rn(o.y, c, e.y)));
+    v = make_float2(__fmaf_rn(2.0f, e.x, -u.x), __fmaf_rn(2.0f, e.y, -u.y));
+  }
+}
+
 // In-register R-point DFT (R = 1..32), recursive radix-2 decimation in time:
 // DFT_R(a) from DFT_{R/2} of the even and odd samples.  Every index is affine
 // in unrolled loop counters, so the whole transform stays in registers.
@@ -64,11 +87,7 @@ struct Dft {
     Dft<H, DIR>::run(e);
     Dft<H, DIR>::run(o);
 #pragma unroll
-    for (int k = 0; k < H; ++k) {
-      const float2 t = twmul32<DIR>(o[k], k * (32 / R));
-      a[k] = cadd(e[k], t);
-      a[k + H] = csub(e[k], t);
-    }
+    for (int k = 0; k < H; ++k) bfly32<DIR>(e[k], o[k], k * (32 / R), a[k], a[k + H]);
   }
 };
 template <int DIR>
