@@ -105,6 +105,33 @@ struct Dft<2, DIR> {
 template <int R, int DIR>
 __device__ __forceinline__ void dft(float2* a) { Dft<R, DIR>::run(a); }
 
+// The same DFT with its first radix-2 level left to the caller: element i of
+// `a` is input OFF + i STRIDE of the whole transform, and each two-point leaf
+// calls leaf(i0, i1, x0, x1, u, v), i1 = i0 + R/2, which must set u = x0' + x1'
+// and v = x0' - x1' for its own scaled inputs x' (e.g. x times a twiddle).
+template <int R, int DIR, int STRIDE = 1, int OFF = 0>
+struct DftLeaf {
+  template <class Leaf>
+  static __device__ __forceinline__ void run(float2* a, Leaf& leaf) {
+    constexpr int H = R / 2;
+    float2 e[H], o[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) { e[i] = a[2 * i]; o[i] = a[2 * i + 1]; }
+    DftLeaf<H, DIR, 2 * STRIDE, OFF>::run(e, leaf);
+    DftLeaf<H, DIR, 2 * STRIDE, OFF + STRIDE>::run(o, leaf);
+#pragma unroll
+    for (int k = 0; k < H; ++k) bfly32<DIR>(e[k], o[k], k * (32 / R), a[k], a[k + H]);
+  }
+};
+template <int DIR, int STRIDE, int OFF>
+struct DftLeaf<2, DIR, STRIDE, OFF> {
+  template <class Leaf>
+  static __device__ __forceinline__ void run(float2* a, Leaf& leaf) {
+    const float2 x0 = a[0], x1 = a[1];
+    leaf(OFF, OFF + STRIDE, x0, x1, a[0], a[1]);
+  }
+};
+
 // Shared-memory index with one pad slot per 16 float2: radix-R scatters at
 // stride R (R <= 16) then land in distinct 8-byte banks of a half warp.
 __device__ __forceinline__ int padx(int a) { return a + (a >> 4); }
