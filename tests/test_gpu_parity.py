@@ -282,6 +282,36 @@ def test_graph_replay_matches_direct_launches():
     mix.set_timing(False)
 
 
+@pytest.mark.parametrize("wl", ["c3", "c4", "c5"])
+def test_dependent_launches_repeatable(wl):
+    """In the batched graph every kernel after the first is a programmatic
+    dependent launch: its CTAs start as the previous kernel's CTAs exit, claim
+    tiles and stage metadata, and wait on the device for that kernel's writes;
+    the forward kernel zeroes the tile cursors.  Over a dozen calls (two-pass
+    forward FFTs, real and complex input) the graph's channel outputs and
+    spectra must equal bit for bit those of the same plan launching stage by
+    stage with stage timing on."""
+    w = workloads.WORKLOADS[wl]()
+    nb = 12
+    stream = workloads.stream_torch(w, nb * w.samples_per_buffer, "cuda:0")
+    rb = w.samples_per_buffer * w.bytes_per_sample
+    plans = [Plan(w.fs, w.fft_size, w.fmt, w.filters(), fc_in=w.fc, ffts_per_buf=w.ffts_per_buf,
+                  averages=w.averages, spectrum_format="f32", mode="batched") for _ in range(2)]
+    plans[1].set_timing(True)
+    bufs = [([torch.empty(c["out_samples"], dtype=torch.complex64, device="cuda") for c in p.channels],
+             torch.empty(p.max_spectra * p.spectrum_bytes, dtype=torch.uint8, device="cuda")) for p in plans]
+    for i in range(nb):
+        raw = stream[i * rb:(i + 1) * rb]
+        r = [p.process_device(raw, o, sp) for p, (o, sp) in zip(plans, bufs)]
+        torch.cuda.synchronize()
+        assert r[0].n_spectra == r[1].n_spectra
+        n = r[0].n_spectra * plans[0].spectrum_bytes
+        assert torch.equal(bufs[0][1][:n], bufs[1][1][:n])
+        for a, b in zip(bufs[0][0], bufs[1][0]):
+            assert torch.equal(a, b), i
+    plans[1].set_timing(False)
+
+
 def test_outputs_stay_inside_their_buffers():
     """Channel outputs are packed into one tensor with sentinel gaps between
     them; after processing every gap still holds its sentinel (n = 4 keeps
