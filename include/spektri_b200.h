@@ -240,7 +240,7 @@ int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_size, int32_t* tile_th
  *         input_format (the N/4 samples carried from the previous window
  *         come first, as in the reference's buffer, main.rs:162-181)
  *   X   : device, n_blocks * K complex64 spectra, K = N/2+1 (real) or N
- * Limit: 8192 + N + n_blocks * Nc <= SK_NOALLOC_SCRATCH_ELEMS (Nc = N/2 for
+ * Limit: 32765 + N + n_blocks * Nc <= SK_NOALLOC_SCRATCH_ELEMS (32765 twiddles; Nc = N/2 for
  * real input, N for complex); larger requests return SK_ERR_ARG.  All calls
  * share the array: calls whose work overlaps on the GPU race.  The first call
  * on each device looks up the array's address and makes synchronous runtime

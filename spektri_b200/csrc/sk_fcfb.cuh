@@ -49,28 +49,30 @@ struct StagePlan {
   static_assert(r0 + r1 + r2 + r3 == LOGN, "stages must cover the transform");
 };
 
-// Powers w^s (s = 1..R-1) of a stage twiddle w = W_8192^(j << SH), conjugated
-// for DIR > 0.  Only w^1, w^4 and w^16 come from the table; the other powers
-// are products of at most three of them (w^(16a + 4b + c) = w^16a w^4b w^c),
-// which keeps each twiddle within a few ulps while cutting the scattered
-// table reads of a radix-R stage from R-1 to at most 3.
+// Powers w^s (s = 1..R-1) of a stage twiddle w = W_P^j, P = 2^(13 - SH) (the
+// stage's span times radix), conjugated for DIR > 0.  Only w^1, w^4 and w^16
+// come from the stage's table (consecutive j at consecutive entries); the
+// other powers are products of at most three of them (w^(16a + 4b + c) =
+// w^16a w^4b w^c), which keeps each twiddle within a few ulps while cutting
+// the table reads of a radix-R stage from R-1 to at most 3.
 template <int R, int SH, int DIR>
 struct TwiddlePowers {
   float2 lo[4], mid[4], hi;                              // w^c (c < 4), w^4b (b < 4), w^16
   __device__ __forceinline__ TwiddlePowers(const float2* __restrict__ tw, int j) {
-    auto ld = [&](int s) {
-      float2 w = __ldg(&tw[(j * s) << SH]);              // forward W_S; inverse uses its conjugate
+    constexpr int p = TILE_LOGS - SH;
+    auto ld = [&](int si) {
+      float2 w = __ldg(&tw[stage_tw_offset(p, si) + j]);  // forward W_P^(j s); inverse uses its conjugate
       if (DIR > 0) w.y = -w.y;
       return w;
     };
-    lo[1] = ld(1);
+    lo[1] = ld(0);
     if constexpr (R > 2) lo[2] = cmul(lo[1], lo[1]);
     if constexpr (R > 3) lo[3] = cmul(lo[2], lo[1]);
-    if constexpr (R > 4) mid[1] = ld(4);
+    if constexpr (R > 4) mid[1] = ld(1);
     if constexpr (R > 8) mid[2] = cmul(mid[1], mid[1]);
     if constexpr (R > 12) mid[3] = cmul(mid[2], mid[1]);
     hi = make_float2(1.f, 0.f);
-    if constexpr (R > 16) hi = ld(16);
+    if constexpr (R > 16) hi = ld(2);
   }
   // w^s for 1 <= s < R (s compile-time after unrolling).
   __device__ __forceinline__ float2 pow(int s) const {
@@ -137,7 +139,7 @@ template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Sto
 __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store,
                                            const Pad& pad = Pad()) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
-  constexpr int SH = TILE_LOGS - LOGL - LOGR;            // tw is the 2^13-point table
+  constexpr int SH = TILE_LOGS - LOGL - LOGR;            // stage tables: P = 2^(LOGL + LOGR)
   static_assert(NB >= 1 && SH >= 0, "bad stage");
   auto twiddled_dft = [&](float2* v, int j) {            // DFT_R(v[s] w^s); no twiddle for LOGL = 0
     if constexpr (LOGL > 0) twiddle_dft<R, SH, DIR>(v, tw, j);

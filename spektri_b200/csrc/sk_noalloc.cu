@@ -51,12 +51,20 @@ struct DeviceSetup {
 std::mutex g_mu;
 std::vector<DeviceSetup> g_setup;
 
-// W_n^k = exp(-2 pi i k / n) for the tile table (n = S) and the window table.
+// W_n^k = exp(-2 pi i k / n) for the tile table (n = S, then the per-stage
+// tables W_P^(j s), layout stage_tw_offset) and the window table.
 __global__ void noalloc_twiddles(float2* tw_tile, float2* tw_big, int n_big) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double s, c;
   if (i < S) {
     sincospi(-2.0 * (double)i / (double)S, &s, &c);
+    tw_tile[i] = make_float2((float)c, (float)s);
+  } else if (i < TILE_TW_ELEMS) {
+    int p = 1;
+    while (p < TILE_LOGS && i >= stage_tw_offset(p + 1, 0)) ++p;
+    const int h = 1 << (p - 1), r = i - stage_tw_offset(p, 0), si = r / h, j = r - si * h;
+    const long long P = 2ll * h, e = ((long long)j * (si == 0 ? 1 : si == 1 ? 4 : 16)) % P;
+    sincospi(-2.0 * (double)e / (double)P, &s, &c);
     tw_tile[i] = make_float2((float)c, (float)s);
   }
   if (i < n_big) {
@@ -111,13 +119,13 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   if ((uintptr_t)raw % (format_bits(input_format) / 8))
     return fail(SK_ERR_ARG, "sk_spectra_noalloc: raw input misaligned for its sample format");
   const long long N = fft_size, Nc = 1ll << log2Nc;
-  const unsigned long long need = (unsigned long long)S + (unsigned long long)N + (unsigned long long)n_blocks * Nc;
+  const unsigned long long need = (unsigned long long)TILE_TW_ELEMS + (unsigned long long)N + (unsigned long long)n_blocks * Nc;
   if (need > kScratchElems)
     return fail(SK_ERR_ARG,
                 "sk_spectra_noalloc: %u blocks of FFT size %u need %llu complex scratch elements; the static "
                 "scratch holds %zu (%zu MiB): at most %lld blocks at this size",
                 n_blocks, fft_size, need, kScratchElems, kScratchElems * sizeof(float2) >> 20,
-                (long long)((kScratchElems - S - N) / Nc));
+                (long long)((kScratchElems - TILE_TW_ELEMS - N) / Nc));
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
@@ -126,10 +134,10 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   float2* tw_tile = base;
-  float2* tw_big = base + S;
-  float2* Z = base + S + N;
+  float2* tw_big = base + TILE_TW_ELEMS;
+  float2* Z = base + TILE_TW_ELEMS + N;
 
-  const int nt = (int)std::max<long long>(S, N);
+  const int nt = (int)std::max<long long>(TILE_TW_ELEMS, N);
   noalloc_twiddles<<<(nt + 255) / 256, 256, 0, st>>>(tw_tile, tw_big, (int)N);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "twiddle kernel: %s", cudaGetErrorString(e));

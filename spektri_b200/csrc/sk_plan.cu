@@ -174,6 +174,22 @@ void twiddles(std::vector<float2>& t, long long n) {
   }
 }
 
+// The tile twiddle array: W_S^k, then the per-stage tables W_P^(j s)
+// (layout: stage_tw_offset).
+void tile_twiddles(std::vector<float2>& t) {
+  twiddles(t, TILE_S);
+  t.resize(TILE_TW_ELEMS);
+  static const int pw[3] = {1, 4, 16};
+  for (int p = 1; p <= TILE_LOGS; ++p) {
+    const long long P = 1ll << p, h = P / 2;
+    for (int si = 0; si < 3; ++si)
+      for (long long j = 0; j < h; ++j) {
+        const double a = -2.0 * M_PI * (double)((j * pw[si]) % P) / (double)P;
+        t[(size_t)(stage_tw_offset(p, si) + j)] = make_float2((float)std::cos(a), (float)std::sin(a));
+      }
+  }
+}
+
 int set_smem_attrs(int fmt) {
   SK_CUDA(fwd_prepare(fmt));
   SK_CUDA(fcfb_prepare());
@@ -580,7 +596,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     if (e != cudaSuccess) { plan_free(pl); return fail(SK_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
   }
   std::vector<float2> tws, twb;
-  twiddles(tws, S);
+  tile_twiddles(tws);
   twiddles(twb, pl->N);
   TRY(dev_alloc(&pl->d_tw_tile, tws.size()));
   TRY(dev_alloc(&pl->d_tw_big, twb.size()));

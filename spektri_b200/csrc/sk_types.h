@@ -12,6 +12,14 @@ constexpr int TILE_S = 8192;              // complex elements per FFT tile
 constexpr int TILE_T = 256;               // threads per tile CTA (32 elements each)
 constexpr int TILE_LOGS = 13;
 constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
+// The tile twiddle array: W_S^k for k < S, then per-stage tables.  A tile FFT
+// stage of span L and radix R (P = L R = 2^p) multiplies by w^s, w = W_P^j,
+// j < L <= P/2; its table holds W_P^(j s) for s = 1, 4, 16 (si = 0, 1, 2) at
+// stage_tw_offset(p, si) + j, so lane-consecutive j read consecutive entries.
+__host__ __device__ constexpr int stage_tw_offset(int p, int si) {
+  return TILE_S + 3 * ((1 << (p - 1)) - 1) + si * (1 << (p - 1));
+}
+constexpr int TILE_TW_ELEMS = TILE_S + 3 * ((1 << TILE_LOGS) - 1);   // p = 1 .. 13
 // Tile in shared memory: S complex values with one pad slot per 16.
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
 // The column pass's tile adds one slot per transform (at most S/16 of them).

@@ -73,7 +73,7 @@ def test_noalloc_allocates_nothing_and_rejects_oversize():
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
-    # 8192 + 65536 + 40 * 32768 complex elements exceed the 8 MiB array
+    # 32765 twiddles + 65536 + 40 * 32768 complex elements exceed the 8 MiB array
     rc = L.sk_spectra_noalloc(raw.data_ptr(), 0x08, N, 40, X.data_ptr(), stream)
     assert rc == SK_ERR_ARG
     msg = last_error()
