@@ -189,7 +189,11 @@ int sk_launches_per_call(const sk_plan* plan);
  * weight design.  X is [B][K] complex64 (the forward FFT of B blocks).
  *   sk_spectra_device : raw -> X for one buffer (advances the halo and the
  *                       Welch state exactly like sk_process_device)
- *   sk_fcfb_forward_device : X, W -> y (W_dev[c] = complex64[n_c] natural order)
+ *   sk_fcfb_forward_device : X, W -> y (W_dev[c] = complex64[n_c] natural order);
+ *                       X is first expanded into the plan's own extended
+ *                       spectrum rows (bin m mod N at every m < N + max n,
+ *                       the filter bank's gather layout), so calls on one plan
+ *                       must stay ordered (one stream, or synchronised)
  *   sk_fcfb_backward_device: X, W, dy -> dW (summed over blocks) and dX
  *                       (accumulated into dX when not NULL); gradients follow
  *                       torch's convention for real losses of complex tensors

@@ -4,11 +4,16 @@
 // A tile holds `count` transforms of n = 2^LOGN points (S/n at most).  The
 // FFT runs as 1-3 Stockham stages (decimation in time, sk_fft.cuh) with the
 // size fixed at compile time:
-//   first stage : load(t, i) supplies input i of transform t (a gather, a
-//                 format conversion, ...), DFT_R, then shared memory (or
-//                 store(t, o, v) directly when it is the only stage)
+//   first stage : load(t, q, s) supplies input i = q + s n/R of transform t
+//                 (a gather, a format conversion, ...), DFT_R, then shared
+//                 memory (or the store directly when it is the only stage)
 //   middle stage: shared -> twiddle -> DFT_R -> shared (in place)
-//   last stage  : shared -> twiddle -> DFT_R -> store(t, o, v) for output o
+//   last stage  : shared -> twiddle -> DFT_R -> store(t, q, u, v) for output
+//                 o = q + u n/R
+// The radix-digit index s (u) is a compile-time constant after unrolling, so a
+// caller can turn index arithmetic on it (the filter bank's n/2 rotation of
+// the inputs, its [n/8, 7n/8) output window) into immediate offsets and
+// statically dropped stores.
 // Shared memory is touched twice per element per middle/last stage; the first
 // and last stages have global memory on their other side, so there is no
 // in-place hazard: the last stage stays rolled over butterflies (one live at a
@@ -47,6 +52,11 @@ struct StagePlan {
                        r2 = stage_log_radix(LOGN, E, 2), r3 = stage_log_radix(LOGN, E, 3);
   static constexpr int ns = (r0 > 0) + (r1 > 0) + (r2 > 0) + (r3 > 0);
   static_assert(r0 + r1 + r2 + r3 == LOGN, "stages must cover the transform");
+  // log2 radix of the last stage, and of the stride n/R between the outputs
+  // q + u n/R that one butterfly of the last stage stores.
+  static constexpr int last = ns == 1 ? r0 : ns == 2 ? r1 : ns == 3 ? r2 : r3;
+  static constexpr int last_shift = LOGN - last;
+  static constexpr int first_shift = LOGN - r0;   // the same stride for the first stage's inputs
 };
 
 // Powers w^s (s = 1..R-1) of a stage twiddle w = W_P^j, P = 2^(13 - SH) (the
@@ -102,8 +112,10 @@ __device__ __forceinline__ void twiddle_dft(float2* v, const float2* __restrict_
   DftLeaf<R, DIR>::run(v, leaf);
 }
 
-// Stage 1 (span L = 1): butterfly q of transform t reads inputs q + s n/R and
-// writes y[q R + u]; as the only stage (n = R, q = 0) it stores output u.
+// Stage 1 (span L = 1): butterfly q of transform t takes inputs
+// i = q + s n/R (load(t, q, s), s = 0..R-1 compile-time after unrolling) and
+// writes y[q R + u]; as the only stage (n = R, q = 0) it stores output u
+// through store(t, 0, u).
 template <int LOGN, int R, int S, int T, int DIR, bool LAST, bool UNROLL, class Load, class Store>
 __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, Store& store) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
@@ -115,7 +127,7 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
     float2 v[R];
     if (t < count) {
 #pragma unroll
-      for (int s = 0; s < R; ++s) v[s] = load(t, q + (s << LOGNR));
+      for (int s = 0; s < R; ++s) v[s] = load(t, q, s);
     } else {
 #pragma unroll
       for (int s = 0; s < R; ++s) v[s] = make_float2(0.f, 0.f);
@@ -124,7 +136,7 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
     if constexpr (LAST) {
       if (t < count) {
 #pragma unroll
-        for (int u = 0; u < R; ++u) store(t, u, v[u]);
+        for (int u = 0; u < R; ++u) store(t, 0, u, v[u]);
       }
     } else {
 #pragma unroll
@@ -134,7 +146,8 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
 }
 
 // Stages 2..: span L = 2^LOGL (LOGL = 0: a first stage run from shared
-// memory, in place).  LAST: q < L, g = 0, output o = q + u L.
+// memory, in place).  LAST: q < L, g = 0, output o = q + u L stored through
+// store(t, q, u, v) (u compile-time after unrolling).
 template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store, class Pad = PadX>
 __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store,
                                            const Pad& pad = Pad()) {
@@ -157,7 +170,7 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
       twiddled_dft(v, q);
       if (t < count) {
 #pragma unroll
-        for (int u = 0; u < R; ++u) store(t, q + (u << LOGNR), v[u]);
+        for (int u = 0; u < R; ++u) store(t, q, u, v[u]);
       }
     }
   } else {
@@ -270,7 +283,7 @@ template <int LOGN, int S, int T, int DIR, class Pad>
 __device__ __forceinline__ void tile_fft_inplace(float2* sm, const float2* __restrict__ tw, const Pad& pad) {
   using P = StagePlan<LOGN, S / T>;
   constexpr int count = S >> LOGN;
-  auto none = [](int, int, float2) {};
+  auto none = [](int, int, int, float2) {};
   stage_next<LOGN, 1 << P::r0, 0, S, T, DIR, false>(sm, count, tw, none, pad);
   if constexpr (P::ns >= 2) {
     __syncthreads();
@@ -287,45 +300,57 @@ __device__ __forceinline__ void tile_fft_inplace(float2* sm, const float2* __res
 }
 
 // ------------------------------------------------------------------ filter bank
+// The filter bank reads the spectra in an extended layout: per block a row of
+// xs >= N + maxn bins holding get_bin(X, N, m) (fftutil.rs:8-22) at every
+// m < xs, i.e. bin m mod N, conjugate-mirrored for real input.  A channel's n
+// bins (first + j) mod N, j < n, are then the contiguous run starting at
+// first mod N, with no modulo, mirror test or select per element.
 struct TileMeta {
-  const float2* X;     // spectrum row of the block, K bins
+  const float2* X;     // extended spectrum row of the block, from bin first mod N
   const float2* w;     // weights, natural order
   float2* out;         // output row of the block: 6(n/8) samples
-  int first;           // first bin modulo N
-  int pad;
+  int pad;             // half tiles: output parity
+  int unused;
 };
 
 struct FcfbTileConst {
-  int N, K;
-  const float2* tw;    // W_8192^k, k < 8192
+  const float2* tw;    // tile twiddle table (W_8192^k, then the stage tables)
 };
 
-// get_bin for the gather: bin m (already reduced modulo N) of one block.
-template <bool REAL>
-__device__ __forceinline__ float2 spectrum_bin(const float2* __restrict__ X, int m, int N, int K) {
-  if constexpr (!REAL) {
-    return __ldg(&X[m]);
-  } else {                                                  // one load, mirror by selects
-    const bool mirror = m >= K;
-    float2 v = __ldg(&X[mirror ? N - m : m]);
-    v.y = mirror ? -v.y : v.y;
-    return v;
+// Weighted input of the IFFT (fcfb.rs:166-172): buf[i] = W[j] bin(first + j),
+// j = (i + n/2) mod n.  With i = q + s n/R (first-stage digit s, q < n/R),
+// j = q + ((s + R/2) mod R) n/R: a compile-time offset from q once s is.
+template <int LOGN, int R>
+__device__ __forceinline__ float2 fcfb_input(const TileMeta& m, int q, int s) {
+  constexpr int LOGNR = LOGN - ilog2c(R);
+  const int j = q + (((s + R / 2) & (R - 1)) << LOGNR);
+  return cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
+}
+
+// Output o = q + u n/R of the last stage lands at o - n/8 when kept
+// ([n/8, 7n/8), fcfb.rs:177).  For R >= 8 the window edges fall on digit
+// boundaries (n/8 = (R/8) n/R), so kept-or-not depends on the compile-time u
+// alone: the dropped quarter costs no test and no store.
+template <int LOGN, int RL, class Emit>
+__device__ __forceinline__ void fcfb_keep(int q, int u, Emit emit) {
+  constexpr int n = 1 << LOGN, lo = n >> 3, keep = 6 * lo, SHL = LOGN - ilog2c(RL);
+  if constexpr (keep > 0) {                                 // n = 4 keeps nothing
+    if constexpr (RL >= 8) {
+      if (u >= RL / 8 && u < 7 * RL / 8) emit(q + ((u - RL / 8) << SHL));
+    } else {
+      const int k = q + (u << SHL) - lo;
+      if ((unsigned)k < (unsigned)keep) emit(k);
+    }
   }
 }
 
-template <int LOGN, int S, int T, bool REAL>
+template <int LOGN, int S, int T>
 __device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c) {
-  constexpr int n = 1 << LOGN, lo = n >> 3, keep = 6 * lo;
-  auto load = [&](int t, int i) {
-    const int j = (i + n / 2) & (n - 1);                    // fcfb.rs:166-169
-    const int m = (meta[t].first + j) & (c.N - 1);
-    return cmul(__ldg(&meta[t].w[j]), spectrum_bin<REAL>(meta[t].X, m, c.N, c.K));
-  };
-  auto store = [&](int t, int o, float2 v) {                // fcfb.rs:177-187
-    if constexpr (keep > 0) {                               // n = 4 keeps nothing
-      o -= lo;
-      if ((unsigned)o < (unsigned)keep) meta[t].out[o] = v;
-    }
+  using P = StagePlan<LOGN, S / T>;
+  constexpr int R0 = 1 << P::r0, RL = 1 << P::last;
+  auto load = [&](int t, int q, int s) { return fcfb_input<LOGN, R0>(meta[t], q, s); };
+  auto store = [&](int t, int q, int u, float2 v) {
+    fcfb_keep<LOGN, RL>(q, u, [&](int k) { meta[t].out[k] = v; });
   };
   tile_pipeline<LOGN, S, T, +1, true>(sm, count, c.tw, load, store);
 }
@@ -337,24 +362,26 @@ __device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int 
 //   y[2k + 1] = IDFT_{n/2}( (buf[i] - buf[i + n/2]) e^{+2 pi i i/n} )[k]
 // so the two halves are independent S-point transforms; each gathers both
 // buf[i] (j = i + n/2) and buf[i + n/2] (j = i) and keeps its parity of
-// [n/8, 7(n/8)).
-template <int S, int T, bool REAL>
+// [n/8, 7(n/8)): y[2o + h] is kept iff o is in [S/8, 7S/8), the same digit
+// window as an S-point transform's.
+template <int S, int T>
 __device__ __forceinline__ void fcfb_tile_half(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
-  constexpr int LOGS = ilog2c(S), n = 2 * S, lo = n >> 3, keep = 6 * lo;
+  constexpr int LOGS = ilog2c(S), n = 2 * S;
   static_assert(n == (1 << TILE_LOGS), "the split twiddle is the 2^13-point table");
+  using P = StagePlan<LOGS, S / T>;
+  constexpr int RL = 1 << P::last;
   const TileMeta& m = meta[0];
   const int h = m.pad;
-  auto load = [&](int, int i) {
-    const int N1 = c.N - 1;
-    const float2 a = cmul(__ldg(&m.w[i + S]), spectrum_bin<REAL>(m.X, (m.first + i + S) & N1, c.N, c.K));
-    const float2 b = cmul(__ldg(&m.w[i]), spectrum_bin<REAL>(m.X, (m.first + i) & N1, c.N, c.K));
+  auto load = [&](int, int q, int s) {
+    const int i = q + (s << P::first_shift);
+    const float2 a = cmul(__ldg(&m.w[i + S]), __ldg(&m.X[i + S]));
+    const float2 b = cmul(__ldg(&m.w[i]), __ldg(&m.X[i]));
     if (h == 0) return cadd(a, b);
     const float2 w = __ldg(&c.tw[i]);                       // e^{-2 pi i i/n}; conjugated below
     return cmul(csub(a, b), make_float2(w.x, -w.y));
   };
-  auto store = [&](int, int o, float2 v) {
-    const int k = 2 * o + h - lo;
-    if ((unsigned)k < (unsigned)keep) m.out[k] = v;
+  auto store = [&](int, int q, int u, float2 v) {       // y[2o + h] at 2o + h - n/8 = 2(o - S/8) + h
+    fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[2 * k + h] = v; });
   };
   tile_pipeline<LOGS, S, T, +1, true>(sm, 1, c.tw, load, store);
 }
@@ -367,62 +394,63 @@ __device__ __forceinline__ void fcfb_tile_half(float2* sm, const TileMeta* meta,
 // [n/8, 7(n/8)) are formed (times c[k]) and stored.  These tiles run in a
 // kernel of their own, so the power-of-two tiles' register allocation is
 // not shaped by them.
-template <int LOGM, int S, int T, bool REAL>
+template <int LOGM, int S, int T>
 __device__ __forceinline__ void fcfb_tile_chirp(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c,
                                                 const BluDesc* __restrict__ bd) {
+  using P = StagePlan<LOGM, S / T>;
   const int n = bd->n, half = n >> 1, lo = n >> 3, keep = 6 * lo;
   const float2* __restrict__ chirp = bd->chirp;
   const float2* __restrict__ H = bd->H;
-  auto load = [&](int t, int i) {
+  auto load = [&](int t, int q, int s) {
+    const int i = q + (s << P::first_shift);
     if (i >= n) return make_float2(0.f, 0.f);
     const int j = i < n - half ? i + half : i - (n - half);  // (i + n/2) mod n, fcfb.rs:166-169
-    const int m = (meta[t].first + j) & (c.N - 1);
-    const float2 x = cmul(__ldg(&meta[t].w[j]), spectrum_bin<REAL>(meta[t].X, m, c.N, c.K));
+    const float2 x = cmul(__ldg(&meta[t].w[j]), __ldg(&meta[t].X[j]));
     return cmul(x, __ldg(&chirp[i]));
   };
-  auto store = [&](int t, int o, float2 v) {
-    const int k = o - lo;
+  auto store = [&](int t, int q, int u, float2 v) {
+    const int o = q + (u << P::last_shift), k = o - lo;
     if ((unsigned)k < (unsigned)keep) meta[t].out[k] = cmul(v, __ldg(&chirp[o]));
   };
   tile_chirp<LOGM, S, T>(sm, count, c.tw, load, H, store);
 }
 
-template <int S, int T, bool REAL, bool CHIRP>
+template <int S, int T, bool CHIRP>
 __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const TileMeta* meta, int count,
                                                    const FcfbTileConst& c, const BluDesc* bd) {
   constexpr int LOGS = ilog2c(S);
   if constexpr (CHIRP) {
     switch (log2n - BLU_TAG) {
-      case 4: fcfb_tile_chirp<4, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 5: fcfb_tile_chirp<5, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 6: fcfb_tile_chirp<6, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 7: fcfb_tile_chirp<7, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 8: fcfb_tile_chirp<8, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 9: fcfb_tile_chirp<9, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 10: fcfb_tile_chirp<10, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 11: fcfb_tile_chirp<11, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 12: if constexpr (LOGS >= 12) fcfb_tile_chirp<12, S, T, REAL>(sm, meta, count, c, bd); break;
-      case 13: if constexpr (LOGS >= 13) fcfb_tile_chirp<13, S, T, REAL>(sm, meta, count, c, bd); break;
+      case 4: fcfb_tile_chirp<4, S, T>(sm, meta, count, c, bd); break;
+      case 5: fcfb_tile_chirp<5, S, T>(sm, meta, count, c, bd); break;
+      case 6: fcfb_tile_chirp<6, S, T>(sm, meta, count, c, bd); break;
+      case 7: fcfb_tile_chirp<7, S, T>(sm, meta, count, c, bd); break;
+      case 8: fcfb_tile_chirp<8, S, T>(sm, meta, count, c, bd); break;
+      case 9: fcfb_tile_chirp<9, S, T>(sm, meta, count, c, bd); break;
+      case 10: fcfb_tile_chirp<10, S, T>(sm, meta, count, c, bd); break;
+      case 11: fcfb_tile_chirp<11, S, T>(sm, meta, count, c, bd); break;
+      case 12: if constexpr (LOGS >= 12) fcfb_tile_chirp<12, S, T>(sm, meta, count, c, bd); break;
+      case 13: if constexpr (LOGS >= 13) fcfb_tile_chirp<13, S, T>(sm, meta, count, c, bd); break;
     }
     return;
   } else {
   if (log2n > LOGS) {
-    if constexpr (LOGS < TILE_LOGS) fcfb_tile_half<S, T, REAL>(sm, meta, c);
+    if constexpr (LOGS < TILE_LOGS) fcfb_tile_half<S, T>(sm, meta, c);
     return;
   }
   switch (log2n) {
-    case 2: fcfb_tile<2, S, T, REAL>(sm, meta, count, c); break;
-    case 3: fcfb_tile<3, S, T, REAL>(sm, meta, count, c); break;
-    case 4: fcfb_tile<4, S, T, REAL>(sm, meta, count, c); break;
-    case 5: fcfb_tile<5, S, T, REAL>(sm, meta, count, c); break;
-    case 6: fcfb_tile<6, S, T, REAL>(sm, meta, count, c); break;
-    case 7: fcfb_tile<7, S, T, REAL>(sm, meta, count, c); break;
-    case 8: fcfb_tile<8, S, T, REAL>(sm, meta, count, c); break;
-    case 9: fcfb_tile<9, S, T, REAL>(sm, meta, count, c); break;
-    case 10: fcfb_tile<10, S, T, REAL>(sm, meta, count, c); break;
-    case 11: fcfb_tile<11, S, T, REAL>(sm, meta, count, c); break;
-    case 12: if constexpr (LOGS >= 12) fcfb_tile<12, S, T, REAL>(sm, meta, count, c); break;
-    case 13: if constexpr (LOGS >= 13) fcfb_tile<13, S, T, REAL>(sm, meta, count, c); break;
+    case 2: fcfb_tile<2, S, T>(sm, meta, count, c); break;
+    case 3: fcfb_tile<3, S, T>(sm, meta, count, c); break;
+    case 4: fcfb_tile<4, S, T>(sm, meta, count, c); break;
+    case 5: fcfb_tile<5, S, T>(sm, meta, count, c); break;
+    case 6: fcfb_tile<6, S, T>(sm, meta, count, c); break;
+    case 7: fcfb_tile<7, S, T>(sm, meta, count, c); break;
+    case 8: fcfb_tile<8, S, T>(sm, meta, count, c); break;
+    case 9: fcfb_tile<9, S, T>(sm, meta, count, c); break;
+    case 10: fcfb_tile<10, S, T>(sm, meta, count, c); break;
+    case 11: fcfb_tile<11, S, T>(sm, meta, count, c); break;
+    case 12: if constexpr (LOGS >= 12) fcfb_tile<12, S, T>(sm, meta, count, c); break;
+    case 13: if constexpr (LOGS >= 13) fcfb_tile<13, S, T>(sm, meta, count, c); break;
   }
   }
 }

@@ -3,6 +3,6 @@
 
 namespace sk {
 
-const void* fcfb_ptr_4096(bool cplx, bool persistent) { return fcfb_ptr<4096, 256, 4, false>(cplx, persistent); }
+const void* fcfb_ptr_4096(bool persistent) { return fcfb_ptr<4096, 256, 4, false>(persistent); }
 
 }  // namespace sk

@@ -3,6 +3,6 @@
 
 namespace sk {
 
-const void* fcfb_ptr_4096_chirp(bool cplx, bool persistent) { return fcfb_ptr<4096, 256, 4, true>(cplx, persistent); }
+const void* fcfb_ptr_4096_chirp(bool persistent) { return fcfb_ptr<4096, 256, 4, true>(persistent); }
 
 }  // namespace sk

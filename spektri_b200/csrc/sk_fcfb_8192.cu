@@ -3,6 +3,6 @@
 
 namespace sk {
 
-const void* fcfb_ptr_8192(bool cplx, bool persistent) { return fcfb_ptr<8192, 256, 2, false>(cplx, persistent); }
+const void* fcfb_ptr_8192(bool persistent) { return fcfb_ptr<8192, 256, 2, false>(persistent); }
 
 }  // namespace sk

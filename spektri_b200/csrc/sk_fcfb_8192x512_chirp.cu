@@ -3,6 +3,6 @@
 
 namespace sk {
 
-const void* fcfb_ptr_8192x512_chirp(bool cplx, bool persistent) { return fcfb_ptr<8192, 512, 2, true>(cplx, persistent); }
+const void* fcfb_ptr_8192x512_chirp(bool persistent) { return fcfb_ptr<8192, 512, 2, true>(persistent); }
 
 }  // namespace sk

@@ -5,13 +5,12 @@
 
 namespace sk {
 
+// The kernels read the extended spectrum layout, the same for real and
+// complex input, so one instance serves both.
 template <int S, int T, int MINB, bool CHIRP>
-const void* fcfb_ptr(bool cplx, bool persistent) {
-  if (persistent)
-    return cplx ? (const void*)fcfb_kernel<S, T, MINB, true, false, CHIRP>
-                : (const void*)fcfb_kernel<S, T, MINB, true, true, CHIRP>;
-  return cplx ? (const void*)fcfb_kernel<S, T, MINB, false, false, CHIRP>
-              : (const void*)fcfb_kernel<S, T, MINB, false, true, CHIRP>;
+const void* fcfb_ptr(bool persistent) {
+  return persistent ? (const void*)fcfb_kernel<S, T, MINB, true, CHIRP>
+                    : (const void*)fcfb_kernel<S, T, MINB, false, CHIRP>;
 }
 
 }  // namespace sk

@@ -79,6 +79,14 @@ cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) 
   return cudaGetLastError();
 }
 
+cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int log2N, float2* Xe, long long xs, int maxn,
+                          cudaStream_t st) {
+  const dim3 g((K + 255) / 256, B);
+  if (cplx) extend_kernel<false><<<g, 256, 0, st>>>(X, K, log2N, Xe, xs, maxn);
+  else extend_kernel<true><<<g, 256, 0, st>>>(X, K, log2N, Xe, xs, maxn);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl) {
   const int bins_per_cta = w.B <= WELCH_BINS_MAX_B ? WELCH_WARP_BINS * WELCH_WARPS : WELCH_WARP_BINS;
   const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
@@ -98,19 +106,17 @@ bool fcfb_shape_ok(int tile_size, int tile_threads) {
          (tile_size == 4096 && tile_threads == 256);
 }
 
-const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp) {
-  if (tile_size == 4096)
-    return chirp ? fcfb_ptr_4096_chirp(cplx, persistent) : fcfb_ptr_4096(cplx, persistent);
-  if (tile_threads == 512)
-    return chirp ? fcfb_ptr_8192x512_chirp(cplx, persistent) : fcfb_ptr_8192x512(cplx, persistent);
-  return chirp ? fcfb_ptr_8192_chirp(cplx, persistent) : fcfb_ptr_8192(cplx, persistent);
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool persistent, bool chirp) {
+  if (tile_size == 4096) return chirp ? fcfb_ptr_4096_chirp(persistent) : fcfb_ptr_4096(persistent);
+  if (tile_threads == 512) return chirp ? fcfb_ptr_8192x512_chirp(persistent) : fcfb_ptr_8192x512(persistent);
+  return chirp ? fcfb_ptr_8192_chirp(persistent) : fcfb_ptr_8192(persistent);
 }
 
 cudaError_t fcfb_prepare() {
   const int shapes[][2] = {{8192, 256}, {8192, 512}, {4096, 256}};
   for (const auto& sh : shapes)
-    for (int k = 0; k < 8; ++k) {
-      const cudaError_t e = cudaFuncSetAttribute(fcfb_kernel_ptr(sh[0], sh[1], k & 1, k & 2, k & 4),
+    for (int k = 0; k < 4; ++k) {
+      const cudaError_t e = cudaFuncSetAttribute(fcfb_kernel_ptr(sh[0], sh[1], k & 1, k & 2),
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcfb_smem(sh[0]));
       if (e != cudaSuccess) return e;
     }
@@ -125,16 +131,16 @@ cudaError_t fcfb_prepare() {
 }
 
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_size, tile_threads, false, true, false),
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fcfb_kernel_ptr(tile_size, tile_threads, true, false),
                                                        tile_threads, fcfb_smem(tile_size));
 }
 
-cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
-                        const FcfbArgs& a, int tile_base, cudaStream_t st, bool pdl) {
+cudaError_t launch_fcfb(bool persistent, bool chirp, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
+                        int tile_base, cudaStream_t st, bool pdl) {
   FcfbArgs args = a;
   int base = tile_base;
   void* params[] = {(void*)&args, (void*)&base};
-  return launch_kernel(fcfb_kernel_ptr(tile_size, tile_threads, cplx, persistent, chirp), dim3(grid), dim3(tile_threads),
+  return launch_kernel(fcfb_kernel_ptr(tile_size, tile_threads, persistent, chirp), dim3(grid), dim3(tile_threads),
                        params, fcfb_smem(tile_size), st, pdl);
 }
 

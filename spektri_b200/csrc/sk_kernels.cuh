@@ -8,12 +8,15 @@
 //   fwd_colreg_kernel /  two-pass forward FFT for Nc = R1 * 8192: column pass
 //   fwd_col_kernel       (registers for R1 <= 8, shared memory above) -> Y,
 //   + fwd_row_kernel     then 8192-point rows -> Z in residue layout
-//   welch_kernel /       Z -> X (K bins, real-input split), the Welch term
-//   welch_bins_kernel    |X[k] - (X[k-1]+X[k+1])/2|^2, its f32 accumulation in
+//   welch_kernel /       Z -> X (K bins, real-input split) written as extended
+//   welch_bins_kernel    rows for the filter bank, the Welch term
+//                        |X[k] - (X[k-1]+X[k+1])/2|^2, its f32 accumulation in
 //                        block order, emission and quantisation of records [spectrum.rs:82-163]
-//   welch_split_kernel   Z -> X only (the differentiable stage, the allocation-free entry)
-//   fcfb_kernel          per channel and block: gather n bins (modulo/mirror),
-//                        times weights, inverse FFT, keep [n/8, 7n/8)        [fcfb.rs:154-188]
+//   welch_split_kernel   Z -> X only, [B][K] (the differentiable stage, the allocation-free entry)
+//   extend_kernel        [B][K] -> extended rows (the differentiable stage's filter bank)
+//   fcfb_kernel          per channel and block: n contiguous bins of the extended row
+//                        (get_bin's modulo and mirror already applied), times weights,
+//                        inverse FFT, keep [n/8, 7n/8)                       [fcfb.rs:154-188]
 //   fcfb_backward_kernel adjoint of fcfb_kernel for weight design
 #pragma once
 #include "sk_types.h"
@@ -95,11 +98,13 @@ __device__ __forceinline__ void fwd_tile_blocks(float2* sm, const FwdArgs& a, co
   const int per = a.per > 0 ? a.per : S >> LOGN;
   const int b0 = tile * per;
   const int count = min(per, a.B - b0);
-  auto load = [&](int t, int j) {
+  using P = StagePlan<LOGN, S / T>;
+  auto load = [&](int t, int q, int s) {
+    const int j = q + (s << P::first_shift);
     float2 z = src.pair((long long)(b0 + t) * a.hop + (CPLX ? j : 2 * j));   // x * scaling/N
     return make_float2(z.x * a.wscale, z.y * a.wscale);
   };
-  auto store = [&](int t, int o, float2 v) { a.Z[((size_t)(b0 + t) << LOGN) + o] = v; };
+  auto store = [&](int t, int q, int u, float2 v) { a.Z[((size_t)(b0 + t) << LOGN) + q + (u << P::last_shift)] = v; };
   tile_pipeline<LOGN, S, T, -1, false>(sm, count, a.tw_tile, load, store);
 }
 
@@ -116,7 +121,9 @@ __device__ __forceinline__ void fwd_tile_split(float2* sm, const FwdArgs& a, con
   float2 rot[R1];                                    // W_R1^{j1 k1}: fixed for the tile
 #pragma unroll
   for (int j1 = 0; j1 < R1; ++j1) rot[j1] = __ldg(&a.tw_big[((j1 * k1) & (R1 - 1)) << shR]);
-  auto load = [&](int, int e) {
+  using P = StagePlan<LOGS, S / T>;
+  auto load = [&](int, int q, int s) {
+    const int e = q + (s << P::first_shift);
     float2 z[R1];
 #pragma unroll
     for (int j1 = 0; j1 < R1; ++j1) {
@@ -130,7 +137,7 @@ __device__ __forceinline__ void fwd_tile_split(float2* sm, const FwdArgs& a, con
     if (k1) acc = cmul(acc, __ldg(&a.tw_big[(e * k1) << shC]));
     return acc;
   };
-  auto store = [&](int, int o, float2 v) { Zb[o] = v; };
+  auto store = [&](int, int q, int u, float2 v) { Zb[q + (u << P::last_shift)] = v; };
   tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
 }
 
@@ -282,8 +289,9 @@ __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* 
   const size_t off = ((size_t)b << a.log2Nc) + ((size_t)k1 << LOGS);
   const float2* Yr = Y + off;
   float2* Zr = a.Z + off;
-  auto load = [&](int, int e) { return __ldg(&Yr[e]); };
-  auto store = [&](int, int o, float2 v) { Zr[o] = v; };
+  using P = StagePlan<LOGS, S / T>;
+  auto load = [&](int, int q, int s) { return __ldg(&Yr[q + (s << P::first_shift)]); };
+  auto store = [&](int, int q, int u, float2 v) { Zr[q + (u << P::last_shift)] = v; };
   tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
 }
 
@@ -328,6 +336,30 @@ __global__ void __launch_bounds__(256) welch_split_kernel(SplitArgs a) {
       a.P[(size_t)b * a.K + k] = __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
     }
   }
+}
+
+// ----------------------------------------------------------------- extended spectra
+// Bin k of a block (k < K: all N bins for complex input, 0..N/2 for real)
+// written into its extended row at every m < N + maxn with m = k mod N, and
+// for real input its conjugate at every m = N - k mod N (0 < k < N/2): the
+// row then holds get_bin(X, N, m) (fftutil.rs:8-22) for each m it has.
+template <bool REAL>
+__device__ __forceinline__ void store_ext(float2* __restrict__ row, int N, int maxn, int k, float2 x) {
+  const int end = N + maxn;
+  for (int m = k; m < end; m += N) row[m] = x;
+  if constexpr (REAL) {
+    if (k > 0 && k < N / 2) {
+      const float2 c = cconj(x);
+      for (int m = N - k; m < end; m += N) row[m] = c;
+    }
+  }
+}
+
+template <bool REAL>
+__global__ void __launch_bounds__(256) extend_kernel(const float2* __restrict__ X, int K, int log2N, float2* Xe,
+                                                     long long xs, int maxn) {
+  const int b = blockIdx.y, k = blockIdx.x * 256 + threadIdx.x;
+  if (k < K) store_ext<REAL>(Xe + (size_t)b * xs, 1 << log2N, maxn, k, __ldg(&X[(size_t)b * K + k]));
 }
 
 // ----------------------------------------------------------------- split + Welch
@@ -386,7 +418,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
       const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
       const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
       if (owner) {
-        X[(size_t)(b0 + i) * s.K + kk] = x1;
+        store_ext<REAL>(X + (size_t)(b0 + i) * a.xs, 1 << s.log2N, a.maxn, kk, x1);
         const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
         terms[i][slot] = __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
       }
@@ -430,7 +462,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
     const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
     const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
     if (owner) {
-      s.X[(size_t)b * s.K + kk] = x1;
+      store_ext<REAL>(s.X + (size_t)b * a.xs, 1 << s.log2N, a.maxn, kk, x1);
       const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
       acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
     }
@@ -447,7 +479,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
 // ----------------------------------------------------------------- filter bank
 // CHIRP: the chirp-z tiles of the list (their own launch); else the
 // power-of-two tiles.
-template <int S, int T, int MINB, bool PERSIST, bool REAL, bool CHIRP>
+template <int S, int T, int MINB, bool PERSIST, bool CHIRP>
 __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base) {
   extern __shared__ float2 sm[];
   __shared__ TileMeta s_meta[MAX_TILE_TRANSFORMS];
@@ -460,7 +492,7 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
     if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.cursor, 1);
   }
   for (int it = 0;; ++it) {
-    const FcfbTileConst c{1 << a.log2N, a.K, a.tw};
+    const FcfbTileConst c{a.tw};
     int tile, next = 0;
     if constexpr (PERSIST) {
       __syncthreads();               // also orders the previous tile's reads before this tile's writes
@@ -479,16 +511,16 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       const bool half = !CHIRP && td.log2n > ilog2c(S);      // entry (channel, 2 block + half)
       const int b = half ? cb.y >> 1 : cb.y;
       TileMeta m;
-      m.X = a.X + (size_t)b * a.K;
+      m.X = a.X + (size_t)b * a.xs + (ch.first & ((1ll << a.log2N) - 1));
       m.w = ch.w;
       m.out = ch.out + (size_t)b * keep;
-      m.first = (int)(ch.first & (long long)(c.N - 1));
       m.pad = half ? (cb.y & 1) : 0;
+      m.unused = 0;
       s_meta[threadIdx.x] = m;
     }
     __syncthreads();
     if (it == 0) pdl_wait();                                  // X from the Welch kernel
-    fcfb_tile_dispatch<S, T, REAL, CHIRP>(td.log2n, sm, s_meta, td.count, c, CHIRP ? a.blu + td.pad : nullptr);
+    fcfb_tile_dispatch<S, T, CHIRP>(td.log2n, sm, s_meta, td.count, c, CHIRP ? a.blu + td.pad : nullptr);
     if constexpr (PERSIST) {
       if (threadIdx.x == 0) s_tile[(it + 1) & 1] = next;
     }

@@ -91,7 +91,9 @@ struct sk_plan {
   int halo_cur = 0;
   float2* d_Z = nullptr;
   float2* d_Y = nullptr;                // column-pass output of the two-pass forward FFT (R1 >= 16)
-  float2* d_X = nullptr;
+  float2* d_X = nullptr;                // [B][xs] extended spectra (the filter bank's gather source)
+  long long xs = 0;                     // extended row: N + maxn bins
+  int maxn = 0;                         // largest IFFT size of the plan's channels
   float* d_acc = nullptr;
   float2* d_w = nullptr;
   BluDesc* d_blu = nullptr;             // chirp-z sizes (one per distinct n)
@@ -265,6 +267,8 @@ SplitArgs split_args(const sk_plan* pl, float2* X) {
 WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
   WelchArgs w{};
   w.s = split_args(pl, X);
+  w.xs = pl->xs;
+  w.maxn = pl->maxn;
   w.acc = pl->d_acc;
   w.B = pl->B;
   w.accn0 = c.accn0;
@@ -368,7 +372,7 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
   a.list = t.d_list;
   a.chans = chans;
   a.X = X;
-  a.K = pl->K;
+  a.xs = pl->xs;
   a.log2N = pl->log2N;
   a.tw = pl->d_tw_tile;
   a.blu = pl->d_blu;
@@ -393,14 +397,14 @@ cudaError_t launch_batched(sk_plan* pl, const FcfbArgs& a0, int size, int thread
   if (t.n_chirp > 0) {
     a.cursor = pl->d_cursor + 1;
     a.ntiles = t.n_chirp;
-    e = launch_fcfb(pl->cplx, true, true, size, threads, std::min(grid, t.n_chirp), a, 0, st, graph);
+    e = launch_fcfb(true, true, size, threads, std::min(grid, t.n_chirp), a, 0, st, graph);
     if (e != cudaSuccess) return e;
   }
   if (t.n_batched > t.n_chirp) {
     a.cursor = pl->d_cursor;
     a.tiles = t.d_tiles + t.n_chirp;
     a.ntiles = t.n_batched - t.n_chirp;
-    e = launch_fcfb(pl->cplx, true, false, size, threads, std::min(grid, a.ntiles), a, 0, st,
+    e = launch_fcfb(true, false, size, threads, std::min(grid, a.ntiles), a, 0, st,
                     graph && t.n_chirp == 0);
   }
   return e;
@@ -414,7 +418,7 @@ int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, c
     SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st, graph));
   } else {
     for (size_t c = 0; c < pl->ch.size(); ++c)
-      SK_CUDA(launch_fcfb(pl->cplx, false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
+      SK_CUDA(launch_fcfb(false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
                           t.plain_start[c], st));
   }
   return SK_OK;
@@ -577,8 +581,13 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     if (filter_status) filter_status[i] = st;
   }
   size_t off = 0;
-  for (auto& c : pl->ch) { c.out_off = off; off += (size_t)pl->B * (c.n / 8 * 6); }
+  for (auto& c : pl->ch) {
+    c.out_off = off;
+    off += (size_t)pl->B * (c.n / 8 * 6);
+    pl->maxn = std::max(pl->maxn, (int)c.n);
+  }
   pl->out_total = off;
+  pl->xs = pl->N + pl->maxn;
 
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
@@ -605,7 +614,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
   TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
   if (pl->R1 > 1) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B << pl->log2Nc));
-  TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->K));
+  TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->xs));
   TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
   TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
   TRY(dev_alloc(&pl->d_chans, pl->ch.size()));
@@ -1002,11 +1011,13 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
     SK_CUDA(cudaStreamSynchronize(st));
   }
   if (pl->ch.empty()) return SK_OK;
-  FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, (const float2*)X);
+  // The caller's [B][K] spectra into the plan's extended rows, then the filter bank.
+  SK_CUDA(launch_extend(pl->cplx, pl->B, (const float2*)X, pl->K, pl->log2N, pl->d_X, pl->xs, pl->maxn, st));
+  FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, pl->d_X);
   const sk_plan::TileSet& t = cur_tiles(pl);
-  if (t.n_chirp > 0) SK_CUDA(launch_fcfb(pl->cplx, false, true, pl->fcfb_size, pl->fcfb_threads, t.n_chirp, a, 0, st));
+  if (t.n_chirp > 0) SK_CUDA(launch_fcfb(false, true, pl->fcfb_size, pl->fcfb_threads, t.n_chirp, a, 0, st));
   if (t.n_batched > t.n_chirp)
-    SK_CUDA(launch_fcfb(pl->cplx, false, false, pl->fcfb_size, pl->fcfb_threads, t.n_batched - t.n_chirp, a,
+    SK_CUDA(launch_fcfb(false, false, pl->fcfb_size, pl->fcfb_threads, t.n_batched - t.n_chirp, a,
                         t.n_chirp, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
@@ -1159,7 +1170,7 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   std::vector<ChanDev> own(pl->h_chans);
   for (size_t c = 0; c < own.size(); ++c) own[c].out = (float2*)pl->d_out_ptrs[c];
   SK_CUDA(cudaMemcpyAsync(pl->d_chans_aux, own.data(), sizeof(ChanDev) * own.size(), cudaMemcpyHostToDevice, st));
-  SK_CUDA(cudaMemsetAsync(pl->d_X, 0, sizeof(float2) * (size_t)pl->B * pl->K, st));
+  SK_CUDA(cudaMemsetAsync(pl->d_X, 0, sizeof(float2) * (size_t)pl->B * pl->xs, st));
   cudaEvent_t e0, e1;
   SK_CUDA(cudaEventCreate(&e0));
   SK_CUDA(cudaEventCreate(&e1));

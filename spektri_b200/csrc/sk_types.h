@@ -88,7 +88,9 @@ struct SplitArgs {
 };
 
 struct WelchArgs {
-  SplitArgs s;                 // Z -> X (P unused)
+  SplitArgs s;                 // Z -> s.X in the filter bank's extended layout (s.P unused)
+  long long xs;                // extended row stride: >= N + maxn bins per block
+  int maxn;                    // largest IFFT size of the plan (the wrap margin past bin N - 1)
   float* acc;                  // [K] running accumulator (carried across buffers)
   int B, accn0, averages, fmt;
   float db_plus;               // -10 log10(averages), computed on the host in f32
@@ -101,8 +103,9 @@ struct FcfbArgs {
   int* cursor;                 // persistent mode: next tile to claim
   const int2* list;            // (channel, block) per transform
   const ChanDev* chans;
-  const float2* X;             // [B][K]
-  int K, log2N;
+  const float2* X;             // [B][xs] extended spectra: bin m mod N (mirrored for real input) at every m < xs
+  long long xs;
+  int log2N;
   const float2* tw;            // W_8192^k, k < 8192
   const BluDesc* blu;          // chirp-z sizes (may be null)
 };
@@ -140,6 +143,9 @@ cudaError_t launch_kernel(const void* fn, dim3 grid, dim3 block, void** params, 
 cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStream_t st, bool pdl = false);
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl = false);
+// [B][K] spectra (the differentiable stage's layout) -> [B][xs] extended rows.
+cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int log2N, float2* Xe, long long xs, int maxn,
+                          cudaStream_t st);
 cudaError_t fcfb_prepare();
 // Filter-bank tile shapes (tile_size, tile_threads): (8192, 256), (8192, 512)
 // and (4096, 256); a 4096-point tile runs an 8192-point transform as two halves.
@@ -147,16 +153,16 @@ bool fcfb_shape_ok(int tile_size, int tile_threads);
 constexpr size_t fcfb_smem(int tile_size) { return sizeof(float2) * (size_t)(tile_size + tile_size / 16); }
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* ctas_per_sm);
 // chirp: the kernel for chirp-z tiles (else power-of-two tiles).
-cudaError_t launch_fcfb(bool cplx, bool persistent, bool chirp, int tile_size, int tile_threads, int grid,
-                        const FcfbArgs& a, int tile_base, cudaStream_t st, bool pdl = false);
-const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool cplx, bool persistent, bool chirp);
+cudaError_t launch_fcfb(bool persistent, bool chirp, int tile_size, int tile_threads, int grid, const FcfbArgs& a,
+                        int tile_base, cudaStream_t st, bool pdl = false);
+const void* fcfb_kernel_ptr(int tile_size, int tile_threads, bool persistent, bool chirp);
 // Per-shape instance tables (sk_fcfb_*.cu).
-const void* fcfb_ptr_8192(bool cplx, bool persistent);
-const void* fcfb_ptr_8192_chirp(bool cplx, bool persistent);
-const void* fcfb_ptr_8192x512(bool cplx, bool persistent);
-const void* fcfb_ptr_8192x512_chirp(bool cplx, bool persistent);
-const void* fcfb_ptr_4096(bool cplx, bool persistent);
-const void* fcfb_ptr_4096_chirp(bool cplx, bool persistent);
+const void* fcfb_ptr_8192(bool persistent);
+const void* fcfb_ptr_8192_chirp(bool persistent);
+const void* fcfb_ptr_8192x512(bool persistent);
+const void* fcfb_ptr_8192x512_chirp(bool persistent);
+const void* fcfb_ptr_4096(bool persistent);
+const void* fcfb_ptr_4096_chirp(bool persistent);
 cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 // kind 0: single-pass forward kernel; 1: shared-memory column pass (R1 >= 16);
