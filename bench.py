@@ -12,10 +12,15 @@ accumulation, and the filter bank (one persistent launch).
           stream over K steps (max over ranks), inputs cycled over more than
           L2 of distinct buffers and outputs (200 MB/step) larger than L2.
   e2e   : the public host API (sk_process): pinned host input copied in, all
-          channel outputs and spectra copied back, every step.
+          channel outputs and spectra copied back, every step; its bound is
+          the pinned device-to-host copy bandwidth, measured and reported.
+  plain_value: the plain per-channel path (one filter-bank launch per
+          channel) on the same buffers; batched_over_plain is the ratio.
   roofline: the filter-bank kernel, algorithmic bytes (its channel outputs)
-          per launch / its event-timed launch duration, against the measured
-          HBM copy bandwidth.
+          per launch / its span inside the batched graph (device timestamps),
+          against the measured HBM copy bandwidth.
+  roofline_pipeline: the whole step's algorithmic bytes (input + channel
+          outputs) / the step time, against the same bandwidth.
   cpu_baseline: the FP32 CPU restatement of the reference path on this host's
           cores, on a bounded sample of the same workload.
 
@@ -153,6 +158,32 @@ def cpu_baseline(w, raws, seconds, threads):
     return n * w.samples_per_buffer / dt, n
 
 
+def workload_config(w, ws):
+    """The workload as both arms report it (identical dicts: the same
+    configuration is measured on the GPU and on the host cores)."""
+    return {"workload": w.name, "input": w.fmt, "fs": w.fs, "fft_size": w.fft_size,
+            "ffts_per_buf": w.ffts_per_buf, "averages": w.averages, "channels": len(w.channels),
+            "sum_ifft_bins": sum(c["n"] for c in w.channels), "samples_per_step": w.samples_per_buffer,
+            "parallelism": f"replicas x{ws}"}
+
+
+def d2h_copy_gbs(dev, nbytes=256 << 20, reps=5):
+    """Pinned device-to-host copy bandwidth (GB/s), best of ``reps`` copies
+    timed with CUDA events: the bound of the host path's output copies."""
+    import torch
+    src = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    dst = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    best = 0.0
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = max(best, nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
+
+
 def run_reference(args, ws, rank):
     """Reference arm: the CPU restatement with all host threads, on this
     workload's configuration; each step one bounded sample (a buffer)."""
@@ -161,6 +192,8 @@ def run_reference(args, ws, rank):
     from spektri_b200 import workloads
     from oracle import oracle32
     w = workloads.WORKLOADS[args.workload]()
+    if args.ffts_per_buf:
+        w.ffts_per_buf = args.ffts_per_buf
     threads = len(os.sched_getaffinity(0))
     per_buf = w.samples_per_buffer
     raw = workloads.stream_numpy(w, 0, 2 * per_buf)
@@ -178,8 +211,7 @@ def run_reference(args, ws, rank):
         "impl": "reference", "metric": "input Msamples/s", "value": round(v, 3), "unit": "Msamples/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": w.name, "fft_size": w.fft_size, "channels": len(w.channels),
-                   "ffts_per_buf": w.ffts_per_buf, "input": w.fmt},
+        "config": workload_config(w, ws),
         "cpu_baseline": {"value": round(v, 3), "unit": "Msamples/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} buffers of {per_buf} samples (FP32 C++ restatement; the Rust "
                                    f"reference needs a Rust toolchain, absent here)"},
@@ -199,7 +231,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--compare-plain", action="store_true", help="also time the plain per-channel path")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip timing the plain per-channel path (one filter-bank launch per channel)")
     ap.add_argument("--ffts-per-buf", type=int, default=0, help="override blocks per buffer (small profiling cases)")
     ap.add_argument("--preroll", type=float, default=1.5, help="seconds of untimed steps while clocks are sampled")
     ap.add_argument("--tuning", default="", help="SIZE,THREADS,CTAS_PER_SM: fixed filter-bank tile shape instead of autotuning")
@@ -272,13 +305,22 @@ def main():
     ms_max = max_over_ranks(ms, ws, local)
     value = args.steps * spb * ws / (ms_max / 1e3) / 1e6       # Msamples/s, all ranks
 
-    # Per-stage event timing (same stream, same work), for the roofline.
-    plan.set_timing(True)
+    # Stage spans in the production path (the same graph and buffers): device
+    # timestamps of each kernel's first start / last end per call.  The
+    # filter bank's span (Welch end -> filter-bank end, the dependent-launch
+    # gap included) is the roofline's launch time.
     kt = min(args.steps, 50)
+    plan.set_trace(True)
+    run_steps(plan, kt, 0)
+    trace_ms, tcalls = plan.trace()
+    plan.set_trace(False)
+    # The same stages launched one by one under CUDA events (no graph, no
+    # dependent launches): a cross-check of the spans.
+    plan.set_timing(True)
     run_steps(plan, kt, 0)
     stage_ms, calls = plan.timing()
     plan.set_timing(False)
-    fcfb_ms = stage_ms[2] / max(1, calls)
+    fcfb_ms = trace_ms[2] / max(1, tcalls)
     out_bytes = sum(c["out_samples"] for c in plan.channels) * 8
     hbm, peak_kind = peaks()
     achieved = out_bytes / (fcfb_ms / 1e3) / 1e9
@@ -302,21 +344,28 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded int16 noise + tones + noise carriers, generated on the GPU)",
-        "config": {"workload": w.name, "mode": args.mode, "input": w.fmt, "fs": w.fs, "fft_size": w.fft_size,
-                   "ffts_per_buf": w.ffts_per_buf, "averages": w.averages, "channels": len(w.channels),
-                   "sum_ifft_bins": sum(c["n"] for c in w.channels), "samples_per_step": spb,
-                   "parallelism": f"replicas x{ws}",
-                   "tuning": {"tile_size": tile_size, "tile_threads": tile_threads, "ctas_per_sm": ctas_per_sm, "fcfb_us": round(tune_us, 1) if tune_us else None,
-                              "source": "fixed" if args.tuning else "autotuned"},
-                   "l2": f"{nbuf} distinct input buffers cycled ({nbuf * raw_bytes / 1e6:.0f} MB) and "
-                         f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2"},
-        "hbm_gbs_pipeline": round(value * 1e6 / ws * alg / 1e9, 1),
+        "config": workload_config(w, ws),
+        "mode": args.mode,
+        "tuning": {"tile_size": tile_size, "tile_threads": tile_threads, "ctas_per_sm": ctas_per_sm,
+                   "fcfb_us": round(tune_us, 1) if tune_us else None, "source": "fixed" if args.tuning else "autotuned"},
+        "l2": f"{nbuf} distinct input buffers cycled ({nbuf * raw_bytes / 1e6:.0f} MB) and "
+              f"{out_bytes / 1e6:.0f} MB of outputs per step, both above the 126 MB L2",
         "alg_bytes_per_sample": round(alg, 3),
-        "stage_ms": {k: round(v / max(1, calls), 4) for k, v in zip(["fwd_fft", "welch", "fcfb"], stage_ms)},
+        # the whole step (forward FFT, Welch, filter bank under the graph):
+        # input bytes + channel-output bytes per sample x samples/s
+        "roofline_pipeline": {"bound": "hbm", "achieved": round(value * 1e6 / ws * alg / 1e9, 1), "peak": hbm,
+                              "unit": "GB/s", "frac": round(value * 1e6 / ws * alg / 1e9 / hbm, 4),
+                              "peak_kind": f"{peak_kind} copy bandwidth",
+                              "alg_bytes_per_step": round(alg * spb)},
+        "stage_ms": {k: round(v / max(1, tcalls), 4) for k, v in zip(["fwd_fft", "welch", "fcfb"], trace_ms)},
+        "stage_ms_source": "device timestamps inside the batched graph (sk_plan_trace), mean over "
+                           f"{tcalls} calls",
+        "stage_ms_direct": {k: round(v / max(1, calls), 4) for k, v in zip(["fwd_fft", "welch", "fcfb"], stage_ms)},
         "roofline": {"bound": "hbm", "kernel": "fcfb_kernel (persistent)", "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "peak_kind": f"{peak_kind} copy bandwidth", "traffic": None,
                      "alg_bytes_per_launch": out_bytes, "launch_ms": round(fcfb_ms, 4),
+                     "launch_ms_source": "filter-bank span in the batched graph (device timestamps)",
                      "fp32": {"flop_per_launch": round(flops), "achieved_tflops": round(flops / (fcfb_ms / 1e3) / 1e12, 2),
                               "peak_tflops": round(fp32_peak, 1), "frac": round(flops / (fcfb_ms / 1e3) / 1e12 / fp32_peak, 4),
                               "peak_kind": "SMs x 128 FP32 lanes x 2 x max SM clock"}},
@@ -329,7 +378,10 @@ def main():
         if d.get("workload") == w.name and d.get("kernel") == "fcfb_kernel":
             result["roofline"]["traffic"] = d.get("dram_bytes_per_launch")
 
-    if args.compare_plain and args.mode == "batched":
+    if not args.no_plain and args.mode == "batched":
+        # The plain per-channel path (the reference's loop over filters,
+        # fcfb.rs:66-100: one filter-bank launch per channel), same tile
+        # shape, same buffers, same events: the batched path's speed-up.
         pp = make("plain")
         pp.set_tuning(tile_size, tile_threads, ctas_per_sm)
         run_steps(pp, args.warmup, 0)
@@ -341,7 +393,8 @@ def main():
         a1.record(st)
         torch.cuda.synchronize(dev)
         vp = kp * spb / (a0.elapsed_time(a1) / 1e3) / 1e6
-        result["plain_value"] = round(vp, 2)
+        result["plain_value"] = round(vp * ws, 2)
+        result["plain_launches_per_step"] = pp.launches_per_call
         result["batched_over_plain"] = round(value / ws / vp, 2)
         del pp
 
@@ -388,8 +441,15 @@ def main():
         d2h += out_bytes + r.n_spectra * plan.spectrum_bytes
     dt = time.perf_counter() - t0
     dt = max_over_ranks(dt, ws, local)
+    d2h_peak = d2h_copy_gbs(dev)
+    d2h_gbs = d2h / dt / 1e9
     result["e2e"] = {"value": round(ke * spb * ws / dt / 1e6, 2), "unit": "Msamples/s",
-                     "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": int(d2h / ke)}
+                     "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": int(d2h / ke),
+                     # the host path copies every channel output back (alg bytes per sample x samples):
+                     # its bound is the pinned device-to-host copy bandwidth, measured here
+                     "d2h_gbs": round(d2h_gbs, 2), "d2h_peak_gbs": round(d2h_peak, 2),
+                     "d2h_frac": round(d2h_gbs / d2h_peak, 4),
+                     "api": "sk_process (pinned host input and outputs, one synchronous call per buffer)"}
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))

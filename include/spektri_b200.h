@@ -216,6 +216,22 @@ int sk_fcfb_backward_device(sk_plan* plan, const float* X, const float* const* W
 int sk_plan_set_timing(sk_plan* plan, int enable);
 int sk_plan_timing(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
 
+/* Stage trace of the production path (the batched CUDA graph included):
+ * every kernel folds the GPU's global timer into per-call slots (first
+ * forward CTA start, last forward / Welch / filter-bank CTA end), which
+ * cost one atomic per CTA and are always recorded.  With tracing enabled,
+ * each sk_process_device call also copies its slots to pinned host memory
+ * and resets them (two small copies after the call on its stream; up to
+ * 4096 calls between reads).  sk_plan_trace waits for the device and
+ * returns, per stage, the summed milliseconds of [forward start, forward
+ * end], [forward end, Welch end] and [Welch end, filter-bank end] (each
+ * stage's span as it runs back to back in the graph, launch gaps
+ * included), the number of calls traced, and resets.  Reference
+ * counterpart: none (the reference has no tracing; scripts wrap runs in
+ * `time`, test/benchmark_spektri.sh:5-6). */
+int sk_plan_set_trace(sk_plan* plan, int enable);
+int sk_plan_trace(sk_plan* plan, double* ms_per_stage, uint64_t* calls);
+
 /* ------------------------------------------------------------ tuning
  * The filter bank runs tiles of tile_size points and tile_threads threads:
  * 8192 x 256 (32 elements per thread), 8192 x 512 (16) or 4096 x 256 (16; an
@@ -241,14 +257,15 @@ int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_size, int32_t* tile_th
  * array of SK_NOALLOC_SCRATCH_ELEMS complex floats (8 MiB) that every GPU
  * loading the library keeps until exit.
  *   raw : device, fft_size/4 + 3*fft_size/4 * n_blocks samples of
- *         input_format (the N/4 samples carried from the previous window
- *         come first, as in the reference's buffer, main.rs:162-181)
+ *         input_format: the last N/4 samples of the previous window, then
+ *         3N/4 * n_blocks new ones; block b is samples [b 3N/4, b 3N/4 + N)
  *   X   : device, n_blocks * K complex64 spectra, K = N/2+1 (real) or N
  * Limit: 32765 + N + n_blocks * Nc <= SK_NOALLOC_SCRATCH_ELEMS (32765 twiddles; Nc = N/2 for
  * real input, N for complex); larger requests return SK_ERR_ARG.  All calls
  * share the array: calls whose work overlaps on the GPU race.  The first call
  * on each device looks up the array's address and makes synchronous runtime
- * calls, so make it before any stream capture. */
+ * calls, so make it before any stream capture; the address is kept for the
+ * process's life, so do not call this on a device after cudaDeviceReset. */
 #define SK_NOALLOC_SCRATCH_ELEMS 1048576
 int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_t fft_size, uint32_t n_blocks,
                        float* X, void* stream);

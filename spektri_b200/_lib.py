@@ -97,6 +97,8 @@ PROTOTYPES = [
     ("sk_plan_get_tuning", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("sk_plan_set_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("sk_plan_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    ("sk_plan_set_trace", C.c_int, [C.c_void_p, C.c_int]),
+    ("sk_plan_trace", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("sk_spectra_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("sk_host_alloc", C.c_void_p, [C.c_size_t]),
     ("sk_host_free", None, [C.c_void_p]),

@@ -309,12 +309,14 @@ struct TileMeta {
   const float2* X;     // extended spectrum row of the block, from bin first mod N
   const float2* w;     // weights, natural order
   float2* out;         // output row of the block: 6(n/8) samples
-  int pad;             // half tiles: output parity
+  int pad;             // split transforms (n > S): the part, i.e. the output residue mod n/S
   int unused;
 };
 
 struct FcfbTileConst {
-  const float2* tw;    // tile twiddle table (W_8192^k, then the stage tables)
+  const float2* tw;        // tile twiddle table (W_8192^k, then the stage tables)
+  const float2* tw_split;  // W_Ns^k, k < Ns = 2^log_split: the twiddles of split transforms (n > S)
+  int log_split;
 };
 
 // Weighted input of the IFFT (fcfb.rs:166-172): buf[i] = W[j] bin(first + j),
@@ -355,33 +357,65 @@ __device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int 
   tile_pipeline<LOGN, S, T, +1, true>(sm, count, c.tw, load, store);
 }
 
-// One half of an n = 2S transform in an S-point tile (count = 1, meta.pad =
-// h).  With buf the shifted, weighted input (buf[i] = W[j] bin(first + j),
-// j = (i + n/2) mod n), the inverse DFT splits by output parity:
-//   y[2k]     = IDFT_{n/2}( buf[i] + buf[i + n/2] )[k]
-//   y[2k + 1] = IDFT_{n/2}( (buf[i] - buf[i + n/2]) e^{+2 pi i i/n} )[k]
-// so the two halves are independent S-point transforms; each gathers both
-// buf[i] (j = i + n/2) and buf[i + n/2] (j = i) and keeps its parity of
-// [n/8, 7(n/8)): y[2o + h] is kept iff o is in [S/8, 7S/8), the same digit
-// window as an S-point transform's.
-template <int S, int T>
-__device__ __forceinline__ void fcfb_tile_half(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
-  constexpr int LOGS = ilog2c(S), n = 2 * S;
-  static_assert(n == (1 << TILE_LOGS), "the split twiddle is the 2^13-point table");
-  using P = StagePlan<LOGS, S / T>;
-  constexpr int RL = 1 << P::last;
+// v times e^{+2 pi i k/P} for a runtime k < P (P <= 8): exact swaps and
+// negations for multiples of a quarter turn, one product otherwise.
+template <int P>
+__device__ __forceinline__ float2 rot_inv(float2 v, int k) {
+  constexpr int Q = P / 4;                                  // k = Q: a quarter turn (P >= 4)
+  if constexpr (P == 2) return k ? make_float2(-v.x, -v.y) : v;
+  if constexpr (P >= 4) {
+    if constexpr (P == 8) {
+      if (k & 1) {                                          // odd eighth turns: times (1 + i)/sqrt(2), then quarter turns
+        const float h = 0.70710678118654752440f;
+        v = make_float2(h * (v.x - v.y), h * (v.x + v.y));
+        k -= 1;
+      }
+    }
+    const int qt = (k / Q) & 3;
+    if (qt == 1) return make_float2(-v.y, v.x);
+    if (qt == 2) return make_float2(-v.x, -v.y);
+    if (qt == 3) return make_float2(v.y, -v.x);
+  }
+  return v;
+}
+
+// One part r of an n = P S transform in an S-point tile (count = 1,
+// meta.pad = r; P = 2, 4, 8).  With buf the shifted, weighted input
+// (buf[i] = W[j] bin(first + j), j = (i + n/2) mod n), the inverse DFT
+// splits by output residue mod P:
+//   y[P k + r] = IDFT_S(z_r)[k],
+//   z_r[i]     = e^{+2 pi i i r/n} sum_m buf[i + m S] e^{+2 pi i m r/P}
+// so the P parts are independent S-point transforms; each gathers all n
+// inputs (buf[i + m S] has j = i + ((m + P/2) mod P) S) and keeps its
+// residue of [n/8, 7(n/8)): y[P k + r] is kept iff k is in [S/8, 7S/8), the
+// same digit window as an S-point transform's, at P (k - S/8) + r.  The
+// twiddle e^{+2 pi i i r/n} is the conjugate of W_n^(i r) from the split
+// table (W_Ns^k, Ns the largest such n of the plan).
+template <int S, int T, int LOGP>
+__device__ __forceinline__ void fcfb_tile_part(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
+  constexpr int LOGS = ilog2c(S), P = 1 << LOGP;
+  using PL = StagePlan<LOGS, S / T>;
+  constexpr int RL = 1 << PL::last;
   const TileMeta& m = meta[0];
-  const int h = m.pad;
+  const int r = m.pad;
+  const int shn = c.log_split - (LOGS + LOGP);              // W_n^k sits at k << shn
   auto load = [&](int, int q, int s) {
-    const int i = q + (s << P::first_shift);
-    const float2 a = cmul(__ldg(&m.w[i + S]), __ldg(&m.X[i + S]));
-    const float2 b = cmul(__ldg(&m.w[i]), __ldg(&m.X[i]));
-    if (h == 0) return cadd(a, b);
-    const float2 w = __ldg(&c.tw[i]);                       // e^{-2 pi i i/n}; conjugated below
-    return cmul(csub(a, b), make_float2(w.x, -w.y));
+    const int i = q + (s << PL::first_shift);
+    float2 z;
+#pragma unroll
+    for (int mm = 0; mm < P; ++mm) {
+      const int j = i + (((mm + P / 2) & (P - 1)) << LOGS);
+      const float2 b = cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
+      z = mm ? cadd(z, rot_inv<P>(b, (mm * r) & (P - 1))) : b;
+    }
+    if (r) {
+      const float2 t = __ldg(&c.tw_split[(i * r) << shn]);
+      z = cmul(z, make_float2(t.x, -t.y));
+    }
+    return z;
   };
-  auto store = [&](int, int q, int u, float2 v) {       // y[2o + h] at 2o + h - n/8 = 2(o - S/8) + h
-    fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[2 * k + h] = v; });
+  auto store = [&](int, int q, int u, float2 v) {
+    fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[P * k + r] = v; });
   };
   tile_pipeline<LOGS, S, T, +1, true>(sm, 1, c.tw, load, store);
 }
@@ -435,7 +469,11 @@ __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const 
     return;
   } else {
   if (log2n > LOGS) {
-    if constexpr (LOGS < TILE_LOGS) fcfb_tile_half<S, T>(sm, meta, c);
+    switch (log2n - LOGS) {
+      case 1: fcfb_tile_part<S, T, 1>(sm, meta, c); break;
+      case 2: fcfb_tile_part<S, T, 2>(sm, meta, c); break;
+      case 3: fcfb_tile_part<S, T, 3>(sm, meta, c); break;
+    }
     return;
   }
   switch (log2n) {

@@ -45,6 +45,20 @@ __device__ __forceinline__ void reset_cursors(int* cursor) {
   }
 }
 
+// Stage trace (sk_types.h TRACE_SLOTS): one thread per CTA folds the global
+// timer into a slot with an atomic min (stage start) or max (stage end).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void trace_start(unsigned long long* trace, int slot) {
+  if (trace && threadIdx.x == 0) atomicMin(trace + slot, global_ns());
+}
+__device__ __forceinline__ void trace_end(unsigned long long* trace, int slot) {
+  if (trace && threadIdx.x == 0) atomicMax(trace + slot, global_ns());
+}
+
 // ----------------------------------------------------------------- input formats
 // One scalar component of a raw sample (inputformats.rs:65-155).  BASE is the
 // format code without its complex bit.
@@ -145,6 +159,7 @@ template <int S, int T, int FMT>
 __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  trace_start(a.trace, 0);
   reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry: convert the last N/4 new samples for the next buffer (main.rs:173)
@@ -177,6 +192,10 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
       case 3: fwd_tile_split<3, S, T, FMT>(sm, a, src, tile); break;
     }
   }
+  if (a.trace) {
+    __syncthreads();
+    trace_end(a.trace, 1);
+  }
 }
 
 // Two-pass forward FFT for Nc = R1 * S with R1 >= 16 (Nc up to 2^21).
@@ -191,6 +210,7 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
   constexpr int E = S / T, LOGS = ilog2c(S);
+  trace_start(a.trace, 0);
   reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry, as in fwd_fft_kernel
@@ -262,6 +282,7 @@ __device__ __forceinline__ void fwd_cols_reg(const FwdArgs& a, const SampleSrc<F
 template <int FMT>
 __global__ void __launch_bounds__(256) fwd_colreg_kernel(FwdArgs a, float2* Y) {
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  trace_start(a.trace, 0);
   reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
   {  // carry, as in fwd_fft_kernel
@@ -293,6 +314,10 @@ __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* 
   auto load = [&](int, int q, int s) { return __ldg(&Yr[q + (s << P::first_shift)]); };
   auto store = [&](int, int q, int u, float2 v) { Zr[q + (u << P::last_shift)] = v; };
   tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
+  if (a.trace) {
+    __syncthreads();
+    trace_end(a.trace, 1);
+  }
 }
 
 // ----------------------------------------------------------------- Welch split
@@ -437,6 +462,7 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
     __syncthreads();
   }
   if (summer) a.acc[kb] = acc;
+  trace_end(a.trace, 2);
 }
 
 // The same records for few blocks per buffer: each warp owns its own 30 bins
@@ -449,31 +475,36 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
   pdl_wait();                                               // Z from the forward FFT
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k0 = (blockIdx.x * WELCH_WARPS + wid) * CB;
-  if (k0 >= a.s.K) return;                                   // whole warp: no shuffle partner left behind
-  const int kk = k0 - 1 + lane;
-  const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
-  const SplitArgs& s = a.s;
-  float acc = owner ? a.acc[kk] : 0.0f;
-  int cnt = a.accn0, r = 0;
+  if (k0 < a.s.K) {                                          // whole warps: no shuffle partner left behind
+    const int kk = k0 - 1 + lane;
+    const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
+    const SplitArgs& s = a.s;
+    float acc = owner ? a.acc[kk] : 0.0f;
+    int cnt = a.accn0, r = 0;
 #pragma unroll 4
-  for (int b = 0; b < a.B; ++b) {
-    const float2* Zb = s.Z + ((size_t)b << s.log2Nc);
-    const float2 x1 = x_at<REAL>(s, Zb, kk);
-    const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
-    const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
-    if (owner) {
-      store_ext<REAL>(s.X + (size_t)b * a.xs, 1 << s.log2N, a.maxn, kk, x1);
-      const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
-      acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
+    for (int b = 0; b < a.B; ++b) {
+      const float2* Zb = s.Z + ((size_t)b << s.log2Nc);
+      const float2 x1 = x_at<REAL>(s, Zb, kk);
+      const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
+      const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
+      if (owner) {
+        store_ext<REAL>(s.X + (size_t)b * a.xs, 1 << s.log2N, a.maxn, kk, x1);
+        const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
+        acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
+      }
+      if (++cnt >= a.averages) {
+        if (owner) emit_record(a, r, kk, acc, cnt);
+        acc = 0.0f;
+        cnt = 0;
+        ++r;
+      }
     }
-    if (++cnt >= a.averages) {
-      if (owner) emit_record(a, r, kk, acc, cnt);
-      acc = 0.0f;
-      cnt = 0;
-      ++r;
-    }
+    if (owner) a.acc[kk] = acc;
   }
-  if (owner) a.acc[kk] = acc;
+  if (a.trace) {
+    __syncthreads();
+    trace_end(a.trace, 2);
+  }
 }
 
 // ----------------------------------------------------------------- filter bank
@@ -492,15 +523,24 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
     if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.cursor, 1);
   }
   for (int it = 0;; ++it) {
-    const FcfbTileConst c{a.tw};
+    const FcfbTileConst c{a.tw, a.tw_split, a.log_split};
     int tile, next = 0;
     if constexpr (PERSIST) {
       __syncthreads();               // also orders the previous tile's reads before this tile's writes
       tile = s_tile[it & 1];
-      if (tile >= a.ntiles) return;
+      if (tile >= a.ntiles) {
+        trace_end(a.trace, 3);
+        return;
+      }
       if (threadIdx.x == 0) next = atomicAdd(a.cursor, 1);
     } else {
-      if (it) return;
+      if (it) {
+        if (a.trace) {
+          __syncthreads();
+          trace_end(a.trace, 3);
+        }
+        return;
+      }
       tile = tile_base + blockIdx.x;
     }
     const TileDesc td = a.tiles[tile];
@@ -508,13 +548,13 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       const int2 cb = __ldg(&a.list[td.list_off + threadIdx.x]);
       const ChanDev& ch = a.chans[cb.x];
       const int keep = 6 * ((CHIRP ? a.blu[td.pad].n : 1 << td.log2n) >> 3);
-      const bool half = !CHIRP && td.log2n > ilog2c(S);      // entry (channel, 2 block + half)
-      const int b = half ? cb.y >> 1 : cb.y;
+      const int logp = CHIRP ? 0 : max(0, td.log2n - ilog2c(S));   // split into 2^logp parts: entry (channel, P block + part)
+      const int b = cb.y >> logp;
       TileMeta m;
       m.X = a.X + (size_t)b * a.xs + (ch.first & ((1ll << a.log2N) - 1));
       m.w = ch.w;
       m.out = ch.out + (size_t)b * keep;
-      m.pad = half ? (cb.y & 1) : 0;
+      m.pad = cb.y & ((1 << logp) - 1);
       m.unused = 0;
       s_meta[threadIdx.x] = m;
     }

@@ -14,20 +14,27 @@
 // The array is g_noalloc_scratch below: SK_NOALLOC_SCRATCH_ELEMS complex
 // floats (8 MiB), reserved on every GPU that loads the library until the
 // process exits.  All calls on a device share it and it keeps whatever the
-// last call left there; every call rewrites the parts it reads (twiddles
-// first, then the FFT results), so nothing has to start at zero.  Two calls
-// whose work overlaps on the GPU (different streams, or different host
-// threads on the same device) race on the array and corrupt each other.
+// last call left there.  Its head holds the twiddle tables: the tile tables
+// (the same for every call) are written by the first call on a device, the
+// window table W_N^k again whenever N differs from the previous call's; the
+// FFT results after them are rewritten by every call, so nothing has to
+// start at zero.  Two calls whose work overlaps on the GPU (different
+// streams, or different host threads on the same device) race on the array
+// and corrupt each other.
 //
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side shadow), so the first call on each device looks up the
 // real address with cudaGetSymbolAddress, with that device current, and sets
 // the kernels' shared-memory limits.  That first call therefore makes
-// synchronous runtime calls; make it before any stream capture begins.
+// synchronous runtime calls; make it before any stream capture begins.  The
+// looked-up address and the table flags are kept per device for the life of
+// the process: do not use this entry point on a device after cudaDeviceReset
+// (the module may load again at another address, and the kernel attributes
+// set here are gone).
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <mutex>
-#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -47,16 +54,20 @@ static __device__ __align__(256) float2 g_noalloc_scratch[kScratchElems];
 struct DeviceSetup {
   bool ready = false;
   float2* base = nullptr;     // device address of g_noalloc_scratch on this device
+  bool tile_tables = false;   // the tile twiddle tables have been written
+  long long window_n = 0;     // N of the window table W_N^k written last (0: none)
 };
 std::mutex g_mu;
-std::vector<DeviceSetup> g_setup;
+std::deque<DeviceSetup> g_setup;      // one per device ordinal; growing it keeps earlier elements in place
 
 // W_n^k = exp(-2 pi i k / n) for the tile table (n = S, then the per-stage
-// tables W_P^(j s), layout stage_tw_offset) and the window table.
-__global__ void noalloc_twiddles(float2* tw_tile, float2* tw_big, int n_big) {
+// tables W_P^(j s), layout stage_tw_offset; skipped when tile == false) and
+// the window table (skipped when n_big == 0).
+__global__ void noalloc_twiddles(float2* tw_tile, float2* tw_big, int n_big, bool tile) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double s, c;
-  if (i < S) {
+  if (!tile) {
+  } else if (i < S) {
     sincospi(-2.0 * (double)i / (double)S, &s, &c);
     tw_tile[i] = make_float2((float)c, (float)s);
   } else if (i < TILE_TW_ELEMS) {
@@ -82,25 +93,30 @@ int log2_exact(long long v) {
 
 // Once per device, with that device current: the array's device address and
 // the kernels' dynamic shared-memory limit.
-int setup_device(int dev, float2** base) {
+DeviceSetup* setup_device(int dev) {
   std::lock_guard<std::mutex> lk(g_mu);
   if ((int)g_setup.size() <= dev) g_setup.resize(dev + 1);
   DeviceSetup& d = g_setup[dev];
   if (!d.ready) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      fail(SK_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+      return nullptr;
+    }
     static const int fmts[] = {SK_FMT_S8, SK_FMT_S16LE, SK_FMT_S16BE, SK_FMT_F32LE, SK_FMT_F32BE, SK_FMT_U8,
                                SK_FMT_CS8, SK_FMT_CS16LE, SK_FMT_CS16BE, SK_FMT_CF32LE, SK_FMT_CF32BE, SK_FMT_CU8};
     for (int f : fmts) {
       e = fwd_prepare(f);
-      if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+      if (e != cudaSuccess) {
+        fail(SK_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        return nullptr;
+      }
     }
     d.base = (float2*)p;
     d.ready = true;
   }
-  *base = d.base;
-  return SK_OK;
+  return &d;
 }
 
 }  // namespace
@@ -129,18 +145,26 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  float2* base = nullptr;
-  int rc = setup_device(dev, &base);
-  if (rc) return rc;
+  DeviceSetup* d = setup_device(dev);
+  if (!d) return SK_ERR_CUDA;
+  float2* base = d->base;
   cudaStream_t st = (cudaStream_t)stream;
   float2* tw_tile = base;
   float2* tw_big = base + TILE_TW_ELEMS;
   float2* Z = base + TILE_TW_ELEMS + N;
 
-  const int nt = (int)std::max<long long>(TILE_TW_ELEMS, N);
-  noalloc_twiddles<<<(nt + 255) / 256, 256, 0, st>>>(tw_tile, tw_big, (int)N);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(SK_ERR_CUDA, "twiddle kernel: %s", cudaGetErrorString(e));
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    const bool tile = !d->tile_tables, window = d->window_n != N;
+    if (tile || window) {               // tables this call reads that the array does not hold yet
+      const int nt = (int)std::max<long long>(tile ? TILE_TW_ELEMS : 0, window ? N : 0);
+      noalloc_twiddles<<<(nt + 255) / 256, 256, 0, st>>>(tw_tile, tw_big, window ? (int)N : 0, tile);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return fail(SK_ERR_CUDA, "twiddle kernel: %s", cudaGetErrorString(e));
+      d->tile_tables = true;
+      d->window_n = N;
+    }
+  }
 
   // The caller's window holds every sample: [N/4 carried | 3N/4 * n_blocks new].
   const long long hop = N - N / 4;

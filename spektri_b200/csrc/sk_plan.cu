@@ -14,6 +14,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "spektri_b200.h"
 #include "sk_internal.h"
@@ -39,6 +40,13 @@ int ilog2_exact(long long v) {
     if (e_ != cudaSuccess)                                                                   \
       return fail(SK_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
+
+// NVTX range over a scope: host-side spans of the API calls and their copy
+// stages, visible to a profiler when one is attached (no cost otherwise).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 // Scoped device selection (restores the caller's current device).
 struct DeviceGuard {
@@ -87,6 +95,8 @@ struct sk_plan {
   // device state
   float2* d_tw_tile = nullptr;
   float2* d_tw_big = nullptr;
+  float2* d_tw_split = nullptr;         // W_Ns^k, k < Ns = 2^log_split: IFFTs split over several tiles
+  int log_split = TILE_LOGS;
   float* d_halo[2] = {nullptr, nullptr};
   int halo_cur = 0;
   float2* d_Z = nullptr;
@@ -133,6 +143,11 @@ struct sk_plan {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraphNode_t node_fwd = nullptr, node_welch = nullptr;
   cudaKernelNodeParams p_fwd{}, p_welch{};
+  // stage trace: device timestamps of every call (sk_types.h TRACE_SLOTS)
+  unsigned long long* d_trace = nullptr;
+  bool tracing = false;
+  unsigned long long* h_trace = nullptr;   // pinned: TRACE_SLOTS per traced call
+  size_t trace_cap = 0, trace_n = 0;
   // stage timing
   bool timing = false;
   std::vector<std::array<cudaEvent_t, SK_N_STAGES + 1>> ev_pending, ev_free;
@@ -145,10 +160,11 @@ namespace {
 int plan_free(sk_plan* pl) {
   if (!pl) return SK_OK;
   DeviceGuard g(pl->p.device);
-  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
+  void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_tw_split, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->ts[0].d_tiles, pl->ts[0].d_list,
                   pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec,
-                  pl->d_blu, pl->d_blu_tab};
+                  pl->d_blu, pl->d_blu_tab, pl->d_trace};
+  if (pl->h_trace) cudaFreeHost(pl->h_trace);
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
   if (pl->graph) cudaGraphDestroy(pl->graph);
   for (void* q : ptrs) if (q) cudaFree(q);
@@ -238,6 +254,7 @@ FwdArgs fwd_args(const sk_plan* pl, const uint8_t* raw) {
   a.tw_big = pl->d_tw_big;
   a.Z = pl->d_Z;
   a.per = pl->fwd_per;
+  a.trace = pl->d_trace;
   return a;
 }
 
@@ -276,6 +293,7 @@ WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
   w.fmt = pl->spec_fmt;
   w.db_plus = pl->db_plus;
   w.out = c.out;
+  w.trace = pl->d_trace;
   return w;
 }
 
@@ -375,7 +393,10 @@ FcfbArgs fcfb_args(sk_plan* pl, const ChanDev* chans, const float2* X) {
   a.xs = pl->xs;
   a.log2N = pl->log2N;
   a.tw = pl->d_tw_tile;
+  a.tw_split = pl->d_tw_split;
+  a.log_split = pl->log_split;
   a.blu = pl->d_blu;
+  a.trace = pl->d_trace;
   return a;
 }
 
@@ -553,12 +574,12 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       fprintf(stderr, "Invalid filter parameters\n");
     } else {
       const int l2 = ilog2_exact(bins);
-      const bool pow2 = l2 >= 2 && l2 <= TILE_LOGS;
+      const bool pow2 = l2 >= 2 && l2 <= MAX_IFFT_LOG;
       const int lm = pow2 ? 0 : chirp_logm(bins);
       if (!pow2 && (bins < 4 || bins % 4 != 0 || lm == 0)) {
         st = SK_ERR_UNSUPPORTED;
         fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two up to %d, "
-                "other multiples of 4 up to 4680)\n", bins, S);
+                "other multiples of 4 up to 4680)\n", bins, 1 << MAX_IFFT_LOG);
       } else {
         sk_plan::Chan c;
         c.n = (uint32_t)bins;
@@ -585,6 +606,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     c.out_off = off;
     off += (size_t)pl->B * (c.n / 8 * 6);
     pl->maxn = std::max(pl->maxn, (int)c.n);
+    pl->log_split = std::max(pl->log_split, c.log2n);
   }
   pl->out_total = off;
   pl->xs = pl->N + pl->maxn;
@@ -609,6 +631,9 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   twiddles(twb, pl->N);
   TRY(dev_alloc(&pl->d_tw_tile, tws.size()));
   TRY(dev_alloc(&pl->d_tw_big, twb.size()));
+  std::vector<float2> twsplit;
+  twiddles(twsplit, 1ll << pl->log_split);
+  TRY(dev_alloc(&pl->d_tw_split, twsplit.size()));
   const size_t halo_n = (size_t)pl->overlap * (cplx ? 2 : 1);
   TRY(dev_alloc(&pl->d_halo[0], halo_n));
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
@@ -621,15 +646,18 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   TRY(dev_alloc(&pl->d_chans_aux, pl->ch.size()));
   TRY(dev_alloc(&pl->d_bwd, pl->ch.size()));
   TRY(dev_alloc(&pl->d_cursor, 2));
+  TRY(dev_alloc(&pl->d_trace, TRACE_SLOTS));
   TRY(dev_alloc(&pl->d_raw, pl->raw_bytes));
   TRY(dev_alloc(&pl->d_out, pl->out_total));
   TRY(dev_alloc(&pl->d_spec, (size_t)pl->max_spectra * pl->K * pl->spec_bin_bytes));
 #define CUDA_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { plan_free(pl); return fail(SK_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); } } while (0)
   CUDA_TRY(cudaMemcpy(pl->d_tw_tile, tws.data(), sizeof(float2) * tws.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(pl->d_tw_big, twb.data(), sizeof(float2) * twb.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(pl->d_tw_split, twsplit.data(), sizeof(float2) * twsplit.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemset(pl->d_halo[0], 0, sizeof(float) * std::max<size_t>(1, halo_n)));   // main.rs:165: zeros
   CUDA_TRY(cudaMemset(pl->d_halo[1], 0, sizeof(float) * std::max<size_t>(1, halo_n)));
   CUDA_TRY(cudaMemset(pl->d_acc, 0, sizeof(float) * pl->K));
+  CUDA_TRY(cudaMemset(pl->d_trace, 0, sizeof(unsigned long long) * TRACE_SLOTS));
   if (!pl->w_host.empty())
     CUDA_TRY(cudaMemcpy(pl->d_w, pl->w_host.data(), sizeof(float) * pl->w_host.size(), cudaMemcpyHostToDevice));
 
@@ -697,13 +725,9 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     std::vector<int2> list;
     std::vector<TileDesc> tiles;
     auto add = [&](int c, int l2) {     // one channel's transforms onto the list
+      const int logp = std::max(0, l2 - logt);                  // split into 2^logp parts (n > tile)
       for (int b = 0; b < pl->B; ++b)
-        if (l2 > logt) {
-          list.push_back(make_int2(c, 2 * b));
-          list.push_back(make_int2(c, 2 * b + 1));
-        } else {
-          list.push_back(make_int2(c, b));
-        }
+        for (int r = 0; r < (1 << logp); ++r) list.push_back(make_int2(c, (b << logp) + r));
     };
     auto per_tile = [&](int l2) { return l2 > logt ? 1 : std::min(t.size >> l2, MAX_TILE_TRANSFORMS); };
     int shrink = 0;                     // batched tiles hold per >> shrink transforms (at least 1)
@@ -715,9 +739,9 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
           for (const auto& c : pl->ch) cnt += (c.log2n == 0 && c.n == (uint32_t)d.n) ? pl->B : 0;
           groups.push_back({cnt, std::min(t.size >> d.logm, MAX_TILE_TRANSFORMS)});
         }
-      for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
+      for (int l2 = MAX_IFFT_LOG; l2 >= 2; --l2) {
         long long cnt = 0;
-        for (const auto& c : pl->ch) cnt += c.log2n == l2 ? (long long)pl->B * (l2 > logt ? 2 : 1) : 0;
+        for (const auto& c : pl->ch) cnt += c.log2n == l2 ? (long long)pl->B << std::max(0, l2 - logt) : 0;
         if (cnt) groups.push_back({cnt, per_tile(l2)});
       }
       for (;; ++shrink) {
@@ -745,7 +769,9 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
           tiles.push_back(TileDesc{BLU_TAG + lm, base + o, std::min(per, cnt - o), (int)k});
       }
     t.n_chirp = (int)tiles.size();
-    for (int l2 = TILE_LOGS; l2 >= 2; --l2) {
+    for (const auto& c : pl->ch)
+      if (c.log2n > logt + MAX_SPLIT_LOG) t.ok = false;         // more parts than a split tile handles
+    for (int l2 = MAX_IFFT_LOG; l2 >= 2; --l2) {
       const int base = (int)list.size();
       for (size_t c = 0; c < pl->ch.size(); ++c)
         if (pl->ch[c].log2n == l2) add((int)c, l2);
@@ -851,6 +877,7 @@ int sk_get_weights(const sk_plan* pl, int32_t c, float* w) {
 int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_out, sk_result* result,
                       void* stream) {
   if (check_plan(pl)) return SK_ERR_ARG;
+  NvtxRange range("sk_process_device");
   if (!raw) return fail(SK_ERR_ARG, "null raw input");
   if (!pl->ch.empty() && !chan_out) return fail(SK_ERR_ARG, "null channel output table");
   const int align = format_bits(pl->fmt) / 8;
@@ -888,6 +915,14 @@ int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void*
     if (rc) return rc;
     if (ev) SK_CUDA(cudaEventRecord((*ev)[3], st));
   }
+  if (pl->tracing && pl->trace_n < pl->trace_cap) {
+    // this call's stage timestamps to the host, then the slots reset for the next call
+    SK_CUDA(cudaMemcpyAsync(pl->h_trace + TRACE_SLOTS * pl->trace_n, pl->d_trace,
+                            sizeof(unsigned long long) * TRACE_SLOTS, cudaMemcpyDeviceToHost, st));
+    SK_CUDA(cudaMemsetAsync(pl->d_trace, 0xFF, sizeof(unsigned long long), st));
+    SK_CUDA(cudaMemsetAsync(pl->d_trace + 1, 0, sizeof(unsigned long long) * (TRACE_SLOTS - 1), st));
+    pl->trace_n += 1;
+  }
   if (result) {
     result->n_spectra = n_spec;
     result->reserved = 0;
@@ -900,6 +935,7 @@ int sk_process_device(sk_plan* pl, const void* raw, void* const* chan_out, void*
 
 int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_out, sk_result* result) {
   if (check_plan(pl)) return SK_ERR_ARG;
+  NvtxRange range("sk_process");
   if (!raw) return fail(SK_ERR_ARG, "null raw input");
   if (!pl->ch.empty() && !chan_out) return fail(SK_ERR_ARG, "null channel output table");
   for (size_t c = 0; c < pl->ch.size(); ++c)
@@ -922,6 +958,7 @@ int sk_process(sk_plan* pl, const void* raw, void* const* chan_out, void* spec_o
     if (!base) base = (const uint8_t*)chan_out[c] - sizeof(float2) * pl->ch[c].out_off;
     else if ((const uint8_t*)chan_out[c] != want) contiguous = false;
   }
+  NvtxRange copy_out("sk_process: outputs to host");
   if (contiguous && base) {
     SK_CUDA(cudaMemcpyAsync((void*)base, pl->d_out, sizeof(float2) * pl->out_total, cudaMemcpyDeviceToHost, st));
   } else {
@@ -1029,6 +1066,9 @@ int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, 
   if (!X || (!pl->ch.empty() && (!W || !dy || !dW))) return fail(SK_ERR_ARG, "null argument");
   if (!pl->h_blu.empty())
     return fail(SK_ERR_UNSUPPORTED, "the adjoint covers power-of-two IFFT sizes; this plan has chirp-z channels");
+  for (const auto& c : pl->ch)
+    if (c.log2n > TILE_LOGS)
+      return fail(SK_ERR_UNSUPPORTED, "the adjoint covers IFFT sizes up to %d; this plan has one of %u", TILE_S, c.n);
   DeviceGuard g(pl->p.device);
   cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
   std::vector<BwdChan> bc(pl->ch.size());
@@ -1087,6 +1127,42 @@ int sk_plan_timing(sk_plan* pl, double* ms, uint64_t* calls) {
   return SK_OK;
 }
 
+int sk_plan_set_trace(sk_plan* pl, int enable) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  DeviceGuard g(pl->p.device);
+  if (enable && !pl->h_trace) {
+    pl->trace_cap = 4096;
+    SK_CUDA(cudaHostAlloc((void**)&pl->h_trace, sizeof(unsigned long long) * TRACE_SLOTS * pl->trace_cap,
+                          cudaHostAllocPortable));
+  }
+  if (enable && !pl->tracing) {                 // slots start empty for the first traced call
+    SK_CUDA(cudaStreamSynchronize(pl->stream));
+    SK_CUDA(cudaDeviceSynchronize());
+    SK_CUDA(cudaMemset(pl->d_trace, 0xFF, sizeof(unsigned long long)));
+    SK_CUDA(cudaMemset(pl->d_trace + 1, 0, sizeof(unsigned long long) * (TRACE_SLOTS - 1)));
+    pl->trace_n = 0;
+  }
+  pl->tracing = enable != 0;
+  return SK_OK;
+}
+
+int sk_plan_trace(sk_plan* pl, double* ms, uint64_t* calls) {
+  if (check_plan(pl)) return SK_ERR_ARG;
+  DeviceGuard g(pl->p.device);
+  SK_CUDA(cudaDeviceSynchronize());             // traced calls may be on any stream
+  double sum[SK_N_STAGES] = {};
+  for (size_t i = 0; i < pl->trace_n; ++i) {
+    const unsigned long long* t = pl->h_trace + TRACE_SLOTS * i;
+    for (int s = 0; s < SK_N_STAGES; ++s)
+      if (t[s + 1] > t[s]) sum[s] += (double)(t[s + 1] - t[s]) * 1e-6;   // ns -> ms; a stage that did not run adds 0
+  }
+  for (int s = 0; s < SK_N_STAGES; ++s)
+    if (ms) ms[s] = sum[s];
+  if (calls) *calls = pl->trace_n;
+  pl->trace_n = 0;
+  return SK_OK;
+}
+
 int sk_plan_set_tuning(sk_plan* pl, int32_t tile_size, int32_t tile_threads, int32_t ctas_per_sm) {
   if (check_plan(pl)) return SK_ERR_ARG;
   if (!fcfb_shape_ok(tile_size, tile_threads))
@@ -1129,7 +1205,7 @@ int sk_plan_autotune(sk_plan* pl, const char* cache_path, double* best_us) {
   // (how many transforms of each IFFT size; FNV-1a of the counts).
   cudaDeviceProp prop{};
   SK_CUDA(cudaGetDeviceProperties(&prop, pl->p.device));
-  int counts[14] = {0};
+  int counts[MAX_IFFT_LOG + 1] = {0};
   for (const auto& c : pl->ch) counts[c.log2n]++;
   unsigned long long h = 1469598103934665603ull;
   for (int v : counts) { h ^= (unsigned long long)v; h *= 1099511628211ull; }

@@ -12,6 +12,8 @@ constexpr int TILE_S = 8192;              // complex elements per FFT tile
 constexpr int TILE_T = 256;               // threads per tile CTA (32 elements each)
 constexpr int TILE_LOGS = 13;
 constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
+constexpr int MAX_SPLIT_LOG = 3;          // an IFFT of up to 2^3 tiles runs as independent parts (n = P S, P <= 8)
+constexpr int MAX_IFFT_LOG = 16;          // power-of-two IFFT sizes up to 2^16
 // The tile twiddle array: W_S^k for k < S, then per-stage tables.  A tile FFT
 // stage of span L and radix R (P = L R = 2^p) multiplies by w^s, w = W_P^j,
 // j < L <= P/2; its table holds W_P^(j s) for s = 1, 4, 16 (si = 0, 1, 2) at
@@ -62,6 +64,13 @@ struct BluDesc {
 };
 constexpr int BLU_TAG = 16;
 
+// Stage trace: global-timer nanoseconds, per call, of [0] the first forward
+// CTA's start (minimum), [1] the last forward CTA's end, [2] the last Welch
+// CTA's end, [3] the last filter-bank CTA's end (maxima).  Recorded by one
+// thread per CTA inside the kernels (also inside the captured graph); the
+// host resets the slots between traced calls.
+constexpr int TRACE_SLOTS = 4;
+
 struct FwdArgs {
   const uint8_t* raw;          // new samples of this buffer
   const float* halo;           // converted last N/4 samples of the previous buffer
@@ -77,6 +86,7 @@ struct FwdArgs {
   int per;                     // Nc <= S: blocks per tile (0: S / Nc, a full tile)
   int* cursor;                 // non-null: the filter bank's two tile cursors, zeroed by the
                                // first forward kernel (the batched graph, in place of a memset)
+  unsigned long long* trace;   // stage trace slots (may be null)
 };
 
 struct SplitArgs {
@@ -95,6 +105,7 @@ struct WelchArgs {
   int B, accn0, averages, fmt;
   float db_plus;               // -10 log10(averages), computed on the host in f32
   uint8_t* out;                // records, K bins each
+  unsigned long long* trace;   // stage trace slots (may be null)
 };
 
 struct FcfbArgs {
@@ -107,7 +118,10 @@ struct FcfbArgs {
   long long xs;
   int log2N;
   const float2* tw;            // W_8192^k, k < 8192
+  const float2* tw_split;      // W_Ns^k, k < Ns = 2^log_split (IFFTs larger than a tile)
+  int log_split;
   const BluDesc* blu;          // chirp-z sizes (may be null)
+  unsigned long long* trace;   // stage trace slots (may be null)
 };
 
 struct BwdArgs {

@@ -10,13 +10,16 @@
 // (dsp.rs:157-158, fcfb.rs:93-95).
 //
 // Additions, all off by default: --spectrumformat=f32, filter keys tw= and w=,
-// --mode=plain|batched (default batched), --device=N and
-// --fake-clock=<secs>,<step_ns> (deterministic timestamps for tests).
+// --mode=plain|batched (default batched), --device=N,
+// --fake-clock=<secs>,<step_ns> (deterministic timestamps for tests) and
+// --stats (at exit, one stderr line with the run's throughput, each
+// pipeline stage's busy time and the device stage spans per buffer).
 #include <cerrno>
 #include <condition_variable>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <cstring>
 #include <ctime>
 #include <mutex>
@@ -137,7 +140,7 @@ int main(int argc, char** argv) {
   bool have_fs = false;
   int fmt = -1;
   std::vector<std::string> filter_strs, binds;
-  bool fake = false;
+  bool fake = false, stats = false;
   unsigned long long clk_secs = 0, clk_step = 0;
 
   auto take = [&](int& i, const std::string& a, const char* lng, const char* sht, std::string& out) -> bool {
@@ -160,6 +163,7 @@ int main(int argc, char** argv) {
   };
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i], v;
+    if (a == "--stats") { stats = true; continue; }
     if (take(i, a, "samplerate", "s", v)) { p.fs_in = parse_f64(v, "samplerate", false); have_fs = true; }
     else if (take(i, a, "centerfreq", "f", v)) p.fc_in = parse_f64(v, "centerfreq", false);
     else if (take(i, a, "fftsize", "n", v)) p.fft_size = (uint32_t)parse_int(v, "fftsize");
@@ -265,6 +269,21 @@ int main(int argc, char** argv) {
   std::mutex mu;
   std::condition_variable cv;
   bool failed = false;
+  // --stats: busy seconds of each pipeline stage, device stage spans
+  using clk = std::chrono::steady_clock;
+  auto secs_since = [](clk::time_point t0) { return std::chrono::duration<double>(clk::now() - t0).count(); };
+  double t_read = 0, t_gpu = 0, t_write = 0, dev_ms[SK_N_STAGES] = {};
+  uint64_t n_done = 0, dev_calls = 0;
+  const clk::time_point t_start = clk::now();
+  auto drain_trace = [&] {
+    double ms[SK_N_STAGES];
+    uint64_t n = 0;
+    if (sk_plan_trace(plan, ms, &n) == SK_OK) {
+      for (int s = 0; s < SK_N_STAGES; ++s) dev_ms[s] += ms[s];
+      dev_calls += n;
+    }
+  };
+  if (stats) sk_plan_set_trace(plan, 1);
   auto wait_state = [&](Slot& sl, int want) {
     std::unique_lock<std::mutex> lk(mu);
     cv.wait(lk, [&] { return failed || sl.state == want || (want == 1 && sl.state == 3); });
@@ -280,7 +299,10 @@ int main(int argc, char** argv) {
     for (uint64_t seq = 0;; ++seq) {
       Slot& sl = slots[seq % NSLOT];
       if (!wait_state(sl, 0)) return;
-      if (!read_exact(sl.raw, raw_bytes)) { set_state(sl, 3); return; }
+      const clk::time_point t0 = clk::now();
+      const bool full = read_exact(sl.raw, raw_bytes);
+      t_read += secs_since(t0);
+      if (!full) { set_state(sl, 3); return; }
       sl.seq = seq;
       if (fake) {
         const unsigned long long t = clk_secs * 1000000000ull + seq * clk_step;
@@ -307,6 +329,7 @@ int main(int argc, char** argv) {
         cv.wait(lk, [&] { return failed || sl.state == 2 || sl.state == 3; });
         if (failed || sl.state == 3) return;
       }
+      const clk::time_point t0 = clk::now();
       for (uint32_t s = 0; s < sl.r.n_spectra; ++s) {
         sk_serialize_metadata(srec.data(), sl.r.spectrum_seq0 + s, sl.secs, sl.nanos);
         std::memcpy(srec.data() + 24, sl.spec + (size_t)s * info.spectrum_bytes, info.spectrum_bytes);
@@ -320,6 +343,7 @@ int main(int argc, char** argv) {
         zmq.send2(outs[c].topic, 24, h, len);
         write_all(outs[c].file, h, len);
       }
+      t_write += secs_since(t0);
       set_state(sl, 0);
     }
   });
@@ -334,7 +358,11 @@ int main(int argc, char** argv) {
       cv.notify_all();
       break;
     }
+    const clk::time_point t0 = clk::now();
     rc = sk_process(plan, sl.raw, sl.payload.data(), sl.spec, &sl.r);
+    t_gpu += secs_since(t0);
+    ++n_done;
+    if (stats && n_done % 1024 == 0) drain_trace();
     if (rc < 0) {
       fprintf(stderr, "spektri: %s\n", sk_last_error());
       exit_code = 1;
@@ -352,6 +380,17 @@ int main(int argc, char** argv) {
   writer.join();
   reader.join();
   fflush(stdout);
+  if (stats) {
+    drain_trace();
+    const double wall = secs_since(t_start), per = dev_calls ? 1e3 / (double)dev_calls : 0.0;
+    const double samples = (double)n_done * (double)info.new_samples;
+    fprintf(stderr,
+            "spektri stats: %llu buffers, %.0f samples in %.3f s = %.2f Msamples/s; busy: stdin %.3f s, "
+            "GPU calls %.3f s, output %.3f s; device per buffer: forward FFT %.1f us, Welch %.1f us, "
+            "filter bank %.1f us\n",
+            (unsigned long long)n_done, samples, wall, wall > 0 ? samples / wall / 1e6 : 0.0, t_read, t_gpu, t_write,
+            dev_ms[0] * per, dev_ms[1] * per, dev_ms[2] * per);
+  }
   for (auto& o : outs)
     if (o.file) fclose(o.file);
   sk_plan_destroy(plan);

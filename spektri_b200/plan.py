@@ -236,6 +236,19 @@ class Plan:
         check(lib().sk_plan_timing(self._h, ms, C.byref(n)), "sk_plan_timing")
         return list(ms), n.value
 
+    def set_trace(self, enable: bool = True):
+        """Trace every following call's stage spans from device timestamps
+        (also inside the batched CUDA graph)."""
+        check(lib().sk_plan_set_trace(self._h, int(bool(enable))))
+
+    def trace(self):
+        """(ms per stage [fwd_fft, welch, fcfb] summed over the traced calls,
+        calls) since the last read: each stage's span in the production path."""
+        ms = (C.c_double * 3)()
+        n = C.c_uint64()
+        check(lib().sk_plan_trace(self._h, ms, C.byref(n)), "sk_plan_trace")
+        return list(ms), n.value
+
     def set_carry(self, raw):
         """Carried samples (the N/4 raw samples before the next buffer), so a
         plan can start mid-stream: a time shard or a restart."""

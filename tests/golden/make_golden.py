@@ -1,9 +1,10 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures under tests/golden/ from the reference tree.
 
-Run in a container that has the reference checked out (default
-/root/reference; override with SPEKTRI_REFERENCE).  The GPU box does not
-have the reference, so the outputs are committed and the tests only read them.
+Run in a container that has the reference checked out, naming its root:
+``python tests/golden/make_golden.py <reference root>`` or with the
+SPEKTRI_REFERENCE environment variable.  The GPU box does not have the
+reference, so the outputs are committed and the tests only read them.
 
 Fixtures:
   kat_two_real_fft.json  the known-answer vectors of spektri/src/dsp/multifft.rs:98-132
@@ -23,7 +24,7 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("SPEKTRI_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPEKTRI_REFERENCE", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -126,6 +127,8 @@ def wire_topics():
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "spektri")):
+        sys.exit("usage: make_golden.py <reference root>  (or set SPEKTRI_REFERENCE): the tejeez/spektri tree")
     with open(os.path.join(OUT, "kat_two_real_fft.json"), "w") as f:
         json.dump(kat_two_real_fft(), f, indent=1)
     with open(os.path.join(OUT, "kat_freq_to_bins.json"), "w") as f:

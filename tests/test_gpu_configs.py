@@ -14,6 +14,7 @@
   one f32 plan and one u8 plan: the averages = 256 record in both formats
   (f32 within 1e-5, u8 within 1 LSB of the FP64 power in dB).
 """
+import glob
 import os
 import subprocess
 
@@ -36,6 +37,15 @@ def _o64(plan, fmt):
     chans = [oracle64.Channel(c["bins"], c["first"], plan.get_weights(i).astype(np.complex128))
              for i, c in enumerate(plan.channels)]
     return oracle64.Oracle64(fmt, plan.fft_size, plan.ffts_per_buf, plan.averages, chans)
+
+
+def _libzmq_env():
+    """The host binary dlopens libzmq: point it at pyzmq's bundled copy."""
+    import zmq
+    base = os.path.dirname(os.path.dirname(zmq.__file__))
+    cands = glob.glob(os.path.join(base, "pyzmq.libs", "libzmq*.so*")) + \
+        glob.glob(os.path.join(os.path.dirname(zmq.__file__), "*libzmq*.so*"))
+    return dict(os.environ, SPEKTRI_LIBZMQ=cands[0] if cands else "")
 
 
 def _records(data, rec_bytes):
@@ -68,7 +78,7 @@ def test_c1_whole_stream_counts_and_parity(tmp_path):
         files = [d / f"c{i}.bin" for i in range(len(filt))]
         args = [binary] + common + ["--zmqbind", f"ipc://{d}/sk.zmq", "--filters"] + \
             [f"{s}:file={p}" for s, p in zip(filt, files)]
-        r = subprocess.run(args, stdin=open(infile, "rb"), capture_output=True, timeout=600)
+        r = subprocess.run(args, stdin=open(infile, "rb"), capture_output=True, timeout=600, env=_libzmq_env())
         assert r.returncode == 0, r.stderr.decode()[-2000:]
         return r.stdout, [p.read_bytes() for p in files]
 

@@ -423,6 +423,40 @@ def test_chirp_sizes_against_oracle(fmt, mode, shape):
     print(f"chirp {fmt} {mode} {shape}: worst rel rms {worst:.2e}")
 
 
+@pytest.mark.parametrize("fmt", ["s16le", "cs16le"])
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+@pytest.mark.parametrize("shape", [(8192, 256, 2), (8192, 512, 2), (4096, 256, 4)])
+def test_ifft_sizes_beyond_a_tile(fmt, mode, shape):
+    """Power-of-two IFFT sizes above the tile size (the reference plans any
+    size, fcfb.rs:150): n = P S runs as P independent S-point parts, one per
+    output residue mod P, up to P = 8 (n = 2^16 on 8192-point tiles, 2^15 on
+    4096-point ones), mixed with small sizes in one plan."""
+    N, B = 65536, 4
+    cplx = oracle64.is_complex(fmt)
+    sizes = [64, 4096, 8192, 16384, 32768] + ([65536] if shape[0] == 8192 else [])
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * ((-1) ** i * (1789 * i + 5) if cplx else 1789 * i + 5))
+               for i, n in enumerate(sizes)]
+    plan = make_plan(N * 1000.0, N, fmt, filters, B, 3, mode=mode)
+    assert [c["bins"] for c in plan.channels] == sizes
+    plan.set_tuning(*shape)
+    rng = np.random.default_rng(41)
+    from tests.test_oracle import _stream
+    worst = run_compare(plan, fmt, [_stream(fmt, plan.new_samples, rng) for _ in range(2)])
+    print(f"split sizes {fmt} {mode} {shape}: worst rel rms {worst:.2e}")
+
+
+def test_split_limits():
+    """2^16-point IFFTs need 8 parts of an 8192-point tile: the 4096-point
+    shape is refused for such a plan, and sizes above 2^16 are dropped."""
+    N = 65536
+    filters = [dict(fs_out=1000.0 * n, fc_out=0.0) for n in (65536, 131072, 64)]
+    plan = make_plan(N * 1000.0, N, "s16le", filters, 2, 3)
+    assert plan.filter_status == [0, SK_ERR_UNSUPPORTED, 0]
+    with pytest.raises(SpektriError):
+        plan.set_tuning(4096, 256, 1)
+    plan.set_tuning(8192, 256, 1)
+
+
 def test_chirp_limits():
     """Sizes whose chirp-z transform exceeds 8192 points are dropped with a
     status; a 4096-point tile shape is refused while a plan holds a chirp-z
