@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--ffts-per-buf", type=int, default=0, help="override blocks per buffer (small profiling cases)")
     ap.add_argument("--preroll", type=float, default=1.5, help="seconds of untimed steps while clocks are sampled")
     ap.add_argument("--tuning", default="", help="SIZE,THREADS,CTAS_PER_SM: fixed filter-bank tile shape instead of autotuning")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time the differentiable forward and the adjoint (always on for c4)")
     ap.add_argument("--by-size", action="store_true",
                     help="also time the filter bank of each IFFT size alone (same tile shape)")
     args = ap.parse_args()
@@ -397,6 +399,41 @@ def main():
         result["plain_launches_per_step"] = pp.launches_per_call
         result["batched_over_plain"] = round(value / ws / vp, 2)
         del pp
+
+    if args.workload == "c4" or args.adjoint:
+        # The differentiable stage on the same buffers: the filter bank as a
+        # separate forward (sk_fcfb_forward_device) and its adjoint
+        # (sk_fcfb_backward_device: dW and dX), input samples per second.
+        K = plan.result_bins
+        X = torch.empty(w.ffts_per_buf, K, dtype=torch.complex64, device=dev)
+        win = torch.empty(plan.total * w.bytes_per_sample, dtype=torch.uint8, device=dev)
+        win[:raw_bytes] = raws[0]
+        win[raw_bytes:] = raws[1][: win.numel() - raw_bytes]
+        plan.spectra_window_device(win, X, stream=st)
+        W = [torch.from_numpy(plan.get_weights(i)).to(dev) for i in range(plan.n_channels)]
+        ys = [torch.empty(c["out_samples"], dtype=torch.complex64, device=dev) for c in plan.channels]
+        dys = [torch.randn(c["out_samples"], dtype=torch.complex64, device=dev) for c in plan.channels]
+        dW = [torch.empty_like(x) for x in W]
+        dX = torch.zeros_like(X)
+        ka = min(args.steps, 50)
+
+        def timed(fn):
+            for _ in range(3):
+                fn()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record(st)
+            for _ in range(ka):
+                fn()
+            b1.record(st)
+            torch.cuda.synchronize(dev)
+            return b0.elapsed_time(b1) / ka
+
+        ms_f = timed(lambda: plan.fcfb_forward_device(X, W, ys, stream=st))
+        ms_b = timed(lambda: plan.fcfb_backward_device(X, W, dys, dW, dX, stream=st))
+        result["differentiable"] = {"fwd_value": round(spb / (ms_f / 1e3) / 1e6, 2),
+                                    "bwd_value": round(spb / (ms_b / 1e3) / 1e6, 2), "unit": "Msamples/s",
+                                    "fwd_ms": round(ms_f, 4), "bwd_ms": round(ms_b, 4),
+                                    "what": "filter bank on one buffer's spectra: forward, and adjoint (dW + dX)"}
 
     if args.by_size:
         # Each IFFT size alone: a plan holding only that size's channels, the

@@ -270,6 +270,27 @@ int sk_plan_get_tuning(const sk_plan* plan, int32_t* tile_size, int32_t* tile_th
 int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_t fft_size, uint32_t n_blocks,
                        float* X, void* stream);
 
+/* ------------------------------------------------------------ rational downconverter
+ * The stage after the filter bank on one channel's complex64 output stream:
+ * mixing with an exact rational oscillator and polyphase resampling by
+ * interpolation / decimation.  Replaces RationalDdc (tools/ddc.py:51-145):
+ * sk_ddc_create is RationalDdc.__init__ (taps designed for input rate x
+ * interpolation, n_taps a multiple of the interpolation; the oscillator is
+ * exp(2 pi i freq_num / freq_den) per sample, freq_den <= 2^24), and
+ * sk_ddc_process_device is RationalDdc.execute: it consumes n_in device
+ * samples and writes the outputs they complete (sk_ddc_outputs tells how many
+ * beforehand: floor(S interpolation / decimation) exist after S samples).
+ * State (FIR history, oscillator and polyphase phases) carries across calls;
+ * one caller thread per object.  DesignDdc (ddc.py:148-177) is
+ * spektri_b200/ddc.py's design_ddc. */
+typedef struct sk_ddc sk_ddc;
+int sk_ddc_create(const float* taps, uint32_t n_taps, uint32_t interpolation, uint32_t decimation, int64_t freq_num,
+                  int64_t freq_den, int32_t device, sk_ddc** out);
+int sk_ddc_outputs(const sk_ddc* ddc, uint64_t n_in, uint64_t* n_out);
+int sk_ddc_process_device(sk_ddc* ddc, const float* in_c64, uint64_t n_in, float* out_c64, uint64_t* n_out,
+                          void* stream);
+void sk_ddc_destroy(sk_ddc* ddc);
+
 /* Pinned host memory for staging (cudaHostAlloc); NULL on failure. */
 void* sk_host_alloc(size_t bytes);
 void sk_host_free(void* p);

@@ -100,6 +100,12 @@ PROTOTYPES = [
     ("sk_plan_set_trace", C.c_int, [C.c_void_p, C.c_int]),
     ("sk_plan_trace", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("sk_spectra_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("sk_ddc_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int64, C.c_int64, C.c_int32,
+                                C.POINTER(C.c_void_p)]),
+    ("sk_ddc_outputs", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("sk_ddc_process_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64),
+                                        C.c_void_p]),
+    ("sk_ddc_destroy", None, [C.c_void_p]),
     ("sk_host_alloc", C.c_void_p, [C.c_size_t]),
     ("sk_host_free", None, [C.c_void_p]),
 ]

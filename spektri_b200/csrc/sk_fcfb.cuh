@@ -393,26 +393,34 @@ __device__ __forceinline__ float2 rot_inv(float2 v, int k) {
 // table (W_Ns^k, Ns the largest such n of the plan).
 template <int S, int T, int LOGP>
 __device__ __forceinline__ void fcfb_tile_part(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
-  constexpr int LOGS = ilog2c(S), P = 1 << LOGP;
+  constexpr int LOGS = ilog2c(S), P = 1 << LOGP, LOGN = LOGS + LOGP;
   using PL = StagePlan<LOGS, S / T>;
   constexpr int RL = 1 << PL::last;
   const TileMeta& m = meta[0];
   const int r = m.pad;
-  const int shn = c.log_split - (LOGS + LOGP);              // W_n^k sits at k << shn
+  // W_n^k: the tile table itself when n = 8192 (compile-time offsets), else
+  // the split table at k << shn
+  const float2* __restrict__ twn = LOGN == TILE_LOGS ? c.tw : c.tw_split;
+  const int shn = LOGN == TILE_LOGS ? 0 : c.log_split - LOGN;
   auto load = [&](int, int q, int s) {
     const int i = q + (s << PL::first_shift);
     float2 z;
+    if constexpr (P == 2) {                                 // y[2k] from buf[i] + buf[i + S], y[2k+1] from the difference
+      const float2 a = cmul(__ldg(&m.w[i + S]), __ldg(&m.X[i + S]));
+      const float2 b = cmul(__ldg(&m.w[i]), __ldg(&m.X[i]));
+      if (r == 0) return cadd(a, b);
+      z = csub(a, b);
+    } else {
 #pragma unroll
-    for (int mm = 0; mm < P; ++mm) {
-      const int j = i + (((mm + P / 2) & (P - 1)) << LOGS);
-      const float2 b = cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
-      z = mm ? cadd(z, rot_inv<P>(b, (mm * r) & (P - 1))) : b;
+      for (int mm = 0; mm < P; ++mm) {
+        const int j = i + (((mm + P / 2) & (P - 1)) << LOGS);
+        const float2 b = cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
+        z = mm ? cadd(z, rot_inv<P>(b, (mm * r) & (P - 1))) : b;
+      }
+      if (r == 0) return z;
     }
-    if (r) {
-      const float2 t = __ldg(&c.tw_split[(i * r) << shn]);
-      z = cmul(z, make_float2(t.x, -t.y));
-    }
-    return z;
+    const float2 t = __ldg(&twn[(i * r) << shn]);
+    return cmul(z, make_float2(t.x, -t.y));
   };
   auto store = [&](int, int q, int u, float2 v) {
     fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[P * k + r] = v; });

@@ -26,8 +26,8 @@ cudaError_t launch_fwd_col_32(int fmt, int grid, const FwdArgs& a, float2* Y, cu
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr_32(int fmt, int kind) {
-#define CASE(F) case F: return fwd_ptr_one<F>(kind);
+const void* fwd_kernel_ptr_32(int fmt, int kind, int R1) {
+#define CASE(F) case F: return fwd_ptr_one<F>(kind, R1);
   switch (fmt) { SK_FOR_FORMATS(CASE) }
 #undef CASE
   return nullptr;

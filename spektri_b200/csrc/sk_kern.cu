@@ -24,11 +24,11 @@ cudaError_t launch_fwd(int fmt, int grid, const FwdArgs& a, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
-const void* fwd_kernel_ptr(int fmt, int kind) {
+const void* fwd_kernel_ptr(int fmt, int kind, int R1) {
   switch (format_bits(fmt)) {
-    case 8: return fwd_kernel_ptr_8(fmt, kind);
-    case 16: return fwd_kernel_ptr_16(fmt, kind);
-    case 32: return fwd_kernel_ptr_32(fmt, kind);
+    case 8: return fwd_kernel_ptr_8(fmt, kind, R1);
+    case 16: return fwd_kernel_ptr_16(fmt, kind, R1);
+    case 32: return fwd_kernel_ptr_32(fmt, kind, R1);
   }
   return nullptr;
 }
@@ -61,29 +61,41 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
   FwdArgs args = a;
   const float2* y = Y;
   void* params[] = {(void*)&args, (void*)&y};
-  return launch_kernel((const void*)fwd_row_kernel<TILE_S, TILE_T>, dim3(grid), dim3(TILE_T), params, TILE_SMEM, st,
+  const void* fn = a.log2R1 < 0 ? (const void*)fwd_rowmix_kernel<TILE_S, TILE_T> : (const void*)fwd_row_kernel<TILE_S, TILE_T>;
+  return launch_kernel(fn, dim3(grid), dim3(TILE_T), params, TILE_SMEM, st,
                        pdl);
 }
 
 // Up to WELCH_BINS_MAX_B blocks per buffer each warp walks its own bins over
 // all blocks; above that the warps of a CTA split the blocks.
-const void* welch_kernel_ptr(bool cplx, int B) {
-  if (B <= WELCH_BINS_MAX_B) return cplx ? (const void*)welch_bins_kernel<false> : (const void*)welch_bins_kernel<true>;
-  return cplx ? (const void*)welch_kernel<false> : (const void*)welch_kernel<true>;
+template <bool P2>
+const void* welch_ptr_t(bool cplx, int B) {
+  if (B <= WELCH_BINS_MAX_B)
+    return cplx ? (const void*)welch_bins_kernel<false, P2> : (const void*)welch_bins_kernel<true, P2>;
+  return cplx ? (const void*)welch_kernel<false, P2> : (const void*)welch_kernel<true, P2>;
+}
+const void* welch_kernel_ptr(bool cplx, int B, bool pow2) {
+  return pow2 ? welch_ptr_t<true>(cplx, B) : welch_ptr_t<false>(cplx, B);
 }
 
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st) {
   const dim3 g((s.K + 255) / 256, B);
-  if (cplx) welch_split_kernel<false><<<g, 256, 0, st>>>(s);
-  else welch_split_kernel<true><<<g, 256, 0, st>>>(s);
+  const bool p2 = (s.N & (s.N - 1)) == 0;
+  if (cplx) {
+    if (p2) welch_split_kernel<false, true><<<g, 256, 0, st>>>(s);
+    else welch_split_kernel<false, false><<<g, 256, 0, st>>>(s);
+  } else {
+    if (p2) welch_split_kernel<true, true><<<g, 256, 0, st>>>(s);
+    else welch_split_kernel<true, false><<<g, 256, 0, st>>>(s);
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int log2N, float2* Xe, long long xs, int maxn,
+cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int N, float2* Xe, long long xs, int maxn,
                           cudaStream_t st) {
   const dim3 g((K + 255) / 256, B);
-  if (cplx) extend_kernel<false><<<g, 256, 0, st>>>(X, K, log2N, Xe, xs, maxn);
-  else extend_kernel<true><<<g, 256, 0, st>>>(X, K, log2N, Xe, xs, maxn);
+  if (cplx) extend_kernel<false><<<g, 256, 0, st>>>(X, K, N, Xe, xs, maxn);
+  else extend_kernel<true><<<g, 256, 0, st>>>(X, K, N, Xe, xs, maxn);
   return cudaGetLastError();
 }
 
@@ -92,7 +104,8 @@ cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pd
   const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
   WelchArgs args = w;
   void* params[] = {(void*)&args};
-  return launch_kernel(welch_kernel_ptr(cplx, w.B), dim3(g), dim3(32 * WELCH_WARPS), params, 0, st, pdl);
+  return launch_kernel(welch_kernel_ptr(cplx, w.B, (w.s.N & (w.s.N - 1)) == 0), dim3(g), dim3(32 * WELCH_WARPS),
+                       params, 0, st, pdl);
 }
 
 // Filter-bank tile shapes (tile size x threads, minimum CTAs per SM):
@@ -120,9 +133,8 @@ cudaError_t fcfb_prepare() {
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcfb_smem(sh[0]));
       if (e != cudaSuccess) return e;
     }
-  const void* fns[] = {(const void*)fcfb_backward_kernel<TILE_S, TILE_T, true>,
-                       (const void*)fcfb_backward_kernel<TILE_S, TILE_T, false>,
-                       (const void*)fwd_row_kernel<TILE_S, TILE_T>};
+  const void* fns[] = {(const void*)fcfb_bwd_fft_kernel<TILE_S, TILE_T>,
+                       (const void*)fwd_row_kernel<TILE_S, TILE_T>, (const void*)fwd_rowmix_kernel<TILE_S, TILE_T>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
     if (e != cudaSuccess) return e;
@@ -144,9 +156,12 @@ cudaError_t launch_fcfb(bool persistent, bool chirp, int tile_size, int tile_thr
                        params, fcfb_smem(tile_size), st, pdl);
 }
 
-cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st) {
-  if (cplx) fcfb_backward_kernel<TILE_S, TILE_T, false><<<grid, TILE_T, TILE_SMEM, st>>>(a);
-  else fcfb_backward_kernel<TILE_S, TILE_T, true><<<grid, TILE_T, TILE_SMEM, st>>>(a);
+cudaError_t launch_fcfb_backward(bool cplx, int grid, int max_n, const BwdArgs& a, cudaStream_t st) {
+  fcfb_bwd_fft_kernel<TILE_S, TILE_T><<<grid, TILE_T, TILE_SMEM, st>>>(a);
+  const dim3 gw((max_n + 255) / 256, a.nchan);
+  if (cplx) fcfb_bwd_dw_kernel<false><<<gw, 256, 0, st>>>(a);
+  else fcfb_bwd_dw_kernel<true><<<gw, 256, 0, st>>>(a);
+  if (a.dX) fcfb_bwd_dx_kernel<0><<<dim3((a.K + 255) / 256, a.B), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 

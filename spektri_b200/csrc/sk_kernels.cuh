@@ -17,7 +17,8 @@
 //   fcfb_kernel          per channel and block: n contiguous bins of the extended row
 //                        (get_bin's modulo and mirror already applied), times weights,
 //                        inverse FFT, keep [n/8, 7n/8)                       [fcfb.rs:154-188]
-//   fcfb_backward_kernel adjoint of fcfb_kernel for weight design
+//   fcfb_bwd_*_kernel    adjoint of fcfb_kernel for weight design (FFT of the output
+//                        gradients, dW and dX sums in a fixed order)
 #pragma once
 #include "sk_types.h"
 #include "sk_fft.cuh"
@@ -52,11 +53,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// Only the first (start) or last (end) TRACE_EDGE CTAs of a grid record, so a
+// kernel of thousands of CTAs adds a few hundred atomics, not thousands; CTAs
+// are dispatched in index order, so the first to start and the last to end
+// are among them.  No barrier: the recording thread stamps its own start or
+// end.
+constexpr int TRACE_EDGE = 512;
 __device__ __forceinline__ void trace_start(unsigned long long* trace, int slot) {
-  if (trace && threadIdx.x == 0) atomicMin(trace + slot, global_ns());
+  if (trace && threadIdx.x == 0 && blockIdx.x < TRACE_EDGE) atomicMin(trace + slot, global_ns());
 }
 __device__ __forceinline__ void trace_end(unsigned long long* trace, int slot) {
-  if (trace && threadIdx.x == 0) atomicMax(trace + slot, global_ns());
+  if (trace && threadIdx.x == 0 && blockIdx.x + TRACE_EDGE >= gridDim.x) atomicMax(trace + slot, global_ns());
 }
 
 // ----------------------------------------------------------------- input formats
@@ -192,10 +199,7 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
       case 3: fwd_tile_split<3, S, T, FMT>(sm, a, src, tile); break;
     }
   }
-  if (a.trace) {
-    __syncthreads();
-    trace_end(a.trace, 1);
-  }
+  trace_end(a.trace, 1);
 }
 
 // Two-pass forward FFT for Nc = R1 * S with R1 >= 16 (Nc up to 2^21).
@@ -301,56 +305,174 @@ __global__ void __launch_bounds__(256) fwd_colreg_kernel(FwdArgs a, float2* Y) {
   }
 }
 
+// Mixed-radix column pass, for the forward sizes that are not powers of two
+// (the reference plans any size, multifft.rs:25-30): Nc = R1 M with
+// R1 = R0 P (R0 = 3 or 5, P = 1, 2, 4) and M = 2^logM <= 8192.  One thread
+// per column j2 < M of one block: the R1-point DFT of z[j1 M + j2] (j1 < R1)
+// in registers, output k1 times W_Nc^(j2 k1), into row k1 of the block's Y
+// (Y[(b R1 + k1) M + j2]); the row pass then gives Z[k1 + R1 k2] at
+// (b R1 + k1) M + k2, the same residue layout as the power-of-two split.
+//
+// R-point DFT, R = R0 P, by Cooley-Tukey with input j = j0 P + j1 and output
+// k = k0 + R0 k1:  X[k0 + R0 k1] = sum_j1 W_P^(j1 k1) W_R^(j1 k0)
+// sum_j0 z[j0 P + j1] W_R0^(j0 k0): direct R0-point sums, twiddles, then the
+// radix-2 Dft<P> per k0.  w[m] = W_R^m (forward sign) for m < R.
+template <int R0, int P>
+__device__ __forceinline__ void mixed_dft(float2* z, const float2* w) {
+  constexpr int R = R0 * P;
+  float2 t[R];
+#pragma unroll
+  for (int j1 = 0; j1 < P; ++j1) {
+#pragma unroll
+    for (int k0 = 0; k0 < R0; ++k0) {
+      float2 acc = z[j1];
+#pragma unroll
+      for (int j0 = 1; j0 < R0; ++j0) {
+        const float2 tw = w[((j0 * k0) % R0) * P];          // W_R0^(j0 k0) = W_R^(j0 k0 P)
+        acc = k0 ? cadd(acc, cmul(z[j0 * P + j1], tw)) : cadd(acc, z[j0 * P + j1]);
+      }
+      t[k0 * P + j1] = (j1 && k0) ? cmul(acc, w[(j1 * k0) % R]) : acc;
+    }
+  }
+#pragma unroll
+  for (int k0 = 0; k0 < R0; ++k0) {
+    dft<P, -1>(t + k0 * P);
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1) z[k0 + R0 * k1] = t[k0 * P + k1];
+  }
+}
+
+template <int R0, int P, int FMT>
+__global__ void __launch_bounds__(256) fwd_colmix_kernel(FwdArgs a, float2* Y) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int R1 = R0 * P;
+  trace_start(a.trace, 0);
+  reset_cursors(a.cursor);
+  const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
+  {  // carry, as in fwd_fft_kernel
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long ncomp = a.overlap * (CPLX ? 2 : 1);
+    const long long base = (a.nnew - a.overlap) * (CPLX ? 2 : 1);
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < ncomp; h += stride)
+      a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
+  }
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ((long long)a.B << a.logM)) return;
+  const int M = 1 << a.logM;
+  const int b = (int)(g >> a.logM), j2 = (int)(g & (M - 1));
+  const long long p0 = (long long)b * a.hop;
+  float2 w[R1];
+  const int nr = a.N / R1;                                   // W_R1^m = W_N^(m N/R1)
+#pragma unroll
+  for (int m = 0; m < R1; ++m) w[m] = __ldg(&a.tw_big[m * nr]);
+  float2 z[R1];
+#pragma unroll
+  for (int j1 = 0; j1 < R1; ++j1) {
+    const int jj = j1 * M + j2;
+    const float2 v = src.pair(p0 + (CPLX ? jj : 2 * jj));
+    z[j1] = make_float2(v.x * a.wscale, v.y * a.wscale);
+  }
+  mixed_dft<R0, P>(z, w);
+  const int step = a.N / a.Nc;                               // W_Nc^k = W_N^(k N/Nc)
+  float2* Yb = Y + (size_t)b * R1 * M + j2;
+  Yb[0] = z[0];
+#pragma unroll
+  for (int k1 = 1; k1 < R1; ++k1) Yb[(size_t)k1 * M] = cmul(z[k1], __ldg(&a.tw_big[j2 * k1 * step]));
+}
+
+// Row pass: the M-point FFT of every row of Y (row r = b R1 + k1 at r M),
+// S/M rows per tile, into Z at the same place (the residue layout).
+template <int LOGM, int S, int T>
+__device__ __forceinline__ void fwd_rows_tile(float2* sm, const FwdArgs& a, const float2* Y, int tile) {
+  constexpr int rpt = S >> LOGM;
+  const int r0 = tile * rpt, count = min(rpt, a.B * a.R1 - r0);
+  const float2* Yr = Y + ((size_t)r0 << LOGM);
+  float2* Zr = a.Z + ((size_t)r0 << LOGM);
+  using P = StagePlan<LOGM, S / T>;
+  auto load = [&](int t, int q, int s) { return __ldg(&Yr[((size_t)t << LOGM) + q + (s << P::first_shift)]); };
+  auto store = [&](int t, int q, int u, float2 v) { Zr[((size_t)t << LOGM) + q + (u << P::last_shift)] = v; };
+  tile_pipeline<LOGM, S, T, -1, false>(sm, count, a.tw_tile, load, store);
+}
+
+// Rows of S points (the power-of-two two-pass FFT) ...
 template <int S, int T>
 __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* Y) {
   extern __shared__ float2 sm[];
-  constexpr int LOGS = ilog2c(S);
   pdl_wait();                                               // Y from the column pass
-  const int b = blockIdx.x >> a.log2R1, k1 = blockIdx.x & (a.R1 - 1);
-  const size_t off = ((size_t)b << a.log2Nc) + ((size_t)k1 << LOGS);
-  const float2* Yr = Y + off;
-  float2* Zr = a.Z + off;
-  using P = StagePlan<LOGS, S / T>;
-  auto load = [&](int, int q, int s) { return __ldg(&Yr[q + (s << P::first_shift)]); };
-  auto store = [&](int, int q, int u, float2 v) { Zr[q + (u << P::last_shift)] = v; };
-  tile_pipeline<LOGS, S, T, -1, false>(sm, 1, a.tw_tile, load, store);
-  if (a.trace) {
-    __syncthreads();
-    trace_end(a.trace, 1);
+  fwd_rows_tile<ilog2c(S), S, T>(sm, a, Y, blockIdx.x);
+  trace_end(a.trace, 1);
+}
+
+// ... and rows of M = 2^logM points, S/M per tile (the mixed-radix FFT).
+template <int S, int T>
+__global__ void __launch_bounds__(T, 2) fwd_rowmix_kernel(FwdArgs a, const float2* Y) {
+  extern __shared__ float2 sm[];
+  pdl_wait();
+  switch (a.logM) {
+    case 4: fwd_rows_tile<4, S, T>(sm, a, Y, blockIdx.x); break;
+    case 5: fwd_rows_tile<5, S, T>(sm, a, Y, blockIdx.x); break;
+    case 6: fwd_rows_tile<6, S, T>(sm, a, Y, blockIdx.x); break;
+    case 7: fwd_rows_tile<7, S, T>(sm, a, Y, blockIdx.x); break;
+    case 8: fwd_rows_tile<8, S, T>(sm, a, Y, blockIdx.x); break;
+    case 9: fwd_rows_tile<9, S, T>(sm, a, Y, blockIdx.x); break;
+    case 10: fwd_rows_tile<10, S, T>(sm, a, Y, blockIdx.x); break;
+    case 11: fwd_rows_tile<11, S, T>(sm, a, Y, blockIdx.x); break;
+    case 12: fwd_rows_tile<12, S, T>(sm, a, Y, blockIdx.x); break;
+    case 13: fwd_rows_tile<13, S, T>(sm, a, Y, blockIdx.x); break;
   }
+  trace_end(a.trace, 1);
 }
 
 // ----------------------------------------------------------------- Welch split
 
+// Packed spectrum element m (the residue layout for R1 > 1).  POW2: N (so Nc
+// and R1) is a power of two: masks and shifts; else R1 = 3, 5, 6, 10, 12 and
+// divisions.  Kernels are instantiated for both, so the power-of-two sizes
+// pay nothing for the others.
+template <bool POW2>
 __device__ __forceinline__ float2 z_at(const SplitArgs& a, const float2* Zb, int m) {
-  return __ldg(&Zb[a.R1 == 1 ? m : ((m & (a.R1 - 1)) << a.logS) + (m >> a.log2R1)]);
+  if (a.R1 == 1) return __ldg(&Zb[m]);
+  if constexpr (POW2) return __ldg(&Zb[((m & (a.R1 - 1)) << a.logM) + (m >> a.log2R1)]);
+  const int k2 = m / a.R1;
+  return __ldg(&Zb[((m - k2 * a.R1) << a.logM) + k2]);
 }
 // Real-input bin k in [0, N/2] from the N/2-point complex FFT of the packed
-// pairs: X = (A + B)/2 - i W_N^k (A - B)/2 with A = Z[k], B = conj(Z[Nc-k]).
+// pairs: X = (A + B)/2 - i W_N^k (A - B)/2 with A = Z[k mod Nc], B = conj(Z[(Nc-k) mod Nc]).
+template <bool POW2>
 __device__ __forceinline__ float2 xr_at(const SplitArgs& a, const float2* Zb, int k) {
-  const int Nc = 1 << a.log2Nc;
-  const float2 za = z_at(a, Zb, k & (Nc - 1));
-  const float2 zb = cconj(z_at(a, Zb, (Nc - k) & (Nc - 1)));
+  float2 za, zb;
+  if constexpr (POW2) {
+    za = z_at<true>(a, Zb, k & (a.Nc - 1));
+    zb = cconj(z_at<true>(a, Zb, (a.Nc - k) & (a.Nc - 1)));
+  } else {
+    za = z_at<false>(a, Zb, k == a.Nc ? 0 : k);
+    zb = cconj(z_at<false>(a, Zb, k == 0 ? 0 : a.Nc - k));
+  }
   const float2 s = cadd(za, zb), d = csub(za, zb);
   const float2 u = cmul(__ldg(&a.tw_big[k]), d);
   return make_float2(0.5f * s.x + 0.5f * u.y, 0.5f * s.y - 0.5f * u.x);
 }
-// get_bin (fftutil.rs:8-22) on the spectrum being formed.
-template <bool REAL>
+// get_bin (fftutil.rs:8-22) on the spectrum being formed, any kk.
+template <bool REAL, bool POW2>
 __device__ __forceinline__ float2 x_at(const SplitArgs& a, const float2* Zb, int kk) {
-  const int N = 1 << a.log2N;
-  const int m = kk & (N - 1);
-  if constexpr (!REAL) return z_at(a, Zb, m);
-  return m < a.K ? xr_at(a, Zb, m) : cconj(xr_at(a, Zb, N - m));
+  int m;
+  if constexpr (POW2) {
+    m = kk & (a.N - 1);
+  } else {
+    m = kk % a.N;
+    m += m < 0 ? a.N : 0;
+  }
+  if constexpr (!REAL) return z_at<POW2>(a, Zb, m);
+  return m < a.K ? xr_at<POW2>(a, Zb, m) : cconj(xr_at<POW2>(a, Zb, a.N - m));
 }
 
-template <bool REAL>
+template <bool REAL, bool POW2>
 __global__ void __launch_bounds__(256) welch_split_kernel(SplitArgs a) {
   __shared__ float2 xs[258];
   const int b = blockIdx.y;
   const int k0 = blockIdx.x * 256;
-  const float2* Zb = a.Z + ((size_t)b << a.log2Nc);
-  for (int idx = threadIdx.x; idx < 258; idx += 256) xs[idx] = x_at<REAL>(a, Zb, k0 - 1 + idx);
+  const float2* Zb = a.Z + (size_t)b * a.Nc;
+  for (int idx = threadIdx.x; idx < 258; idx += 256) xs[idx] = x_at<REAL, POW2>(a, Zb, k0 - 1 + idx);
   __syncthreads();
   const int k = k0 + threadIdx.x;
   if (k < a.K) {
@@ -381,10 +503,10 @@ __device__ __forceinline__ void store_ext(float2* __restrict__ row, int N, int m
 }
 
 template <bool REAL>
-__global__ void __launch_bounds__(256) extend_kernel(const float2* __restrict__ X, int K, int log2N, float2* Xe,
+__global__ void __launch_bounds__(256) extend_kernel(const float2* __restrict__ X, int K, int N, float2* Xe,
                                                      long long xs, int maxn) {
   const int b = blockIdx.y, k = blockIdx.x * 256 + threadIdx.x;
-  if (k < K) store_ext<REAL>(Xe + (size_t)b * xs, 1 << log2N, maxn, k, __ldg(&X[(size_t)b * K + k]));
+  if (k < K) store_ext<REAL>(Xe + (size_t)b * xs, N, maxn, k, __ldg(&X[(size_t)b * K + k]));
 }
 
 // ----------------------------------------------------------------- split + Welch
@@ -416,7 +538,7 @@ __device__ __forceinline__ void emit_record(const WelchArgs& a, int r, int k, fl
   }
 }
 
-template <bool REAL>
+template <bool REAL, bool POW2>
 __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
   constexpr int CB = WELCH_WARP_BINS;                        // bins per CTA (every warp covers them)
   __shared__ float terms[WELCH_CHUNK][CB];
@@ -438,12 +560,12 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
     // Phase A: warp w forms blocks w, w + WARPS, ... (independent loads).
 #pragma unroll 4
     for (int i = wid; i < nb; i += WELCH_WARPS) {
-      const float2* Zb = s.Z + ((size_t)(b0 + i) << s.log2Nc);
-      const float2 x1 = x_at<REAL>(s, Zb, kk);
+      const float2* Zb = s.Z + (size_t)(b0 + i) * s.Nc;
+      const float2 x1 = x_at<REAL, POW2>(s, Zb, kk);
       const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
       const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
       if (owner) {
-        store_ext<REAL>(X + (size_t)(b0 + i) * a.xs, 1 << s.log2N, a.maxn, kk, x1);
+        store_ext<REAL>(X + (size_t)(b0 + i) * a.xs, s.N, a.maxn, kk, x1);
         const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
         terms[i][slot] = __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
       }
@@ -469,42 +591,38 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
 // (+ a 1-bin halo each side) and walks every block in order, accumulating in
 // registers -- the same additions in the same order as welch_kernel's
 // phase B, with no shared memory and no barrier.
-template <bool REAL>
+template <bool REAL, bool POW2>
 __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs a) {
   constexpr int CB = WELCH_WARP_BINS;
   pdl_wait();                                               // Z from the forward FFT
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k0 = (blockIdx.x * WELCH_WARPS + wid) * CB;
-  if (k0 < a.s.K) {                                          // whole warps: no shuffle partner left behind
-    const int kk = k0 - 1 + lane;
-    const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
-    const SplitArgs& s = a.s;
-    float acc = owner ? a.acc[kk] : 0.0f;
-    int cnt = a.accn0, r = 0;
+  if (k0 >= a.s.K) return;                                   // whole warp: no shuffle partner left behind
+  const int kk = k0 - 1 + lane;
+  const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
+  const SplitArgs& s = a.s;
+  float acc = owner ? a.acc[kk] : 0.0f;
+  int cnt = a.accn0, r = 0;
 #pragma unroll 4
-    for (int b = 0; b < a.B; ++b) {
-      const float2* Zb = s.Z + ((size_t)b << s.log2Nc);
-      const float2 x1 = x_at<REAL>(s, Zb, kk);
-      const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
-      const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
-      if (owner) {
-        store_ext<REAL>(s.X + (size_t)b * a.xs, 1 << s.log2N, a.maxn, kk, x1);
-        const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
-        acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
-      }
-      if (++cnt >= a.averages) {
-        if (owner) emit_record(a, r, kk, acc, cnt);
-        acc = 0.0f;
-        cnt = 0;
-        ++r;
-      }
+  for (int b = 0; b < a.B; ++b) {
+    const float2* Zb = s.Z + (size_t)b * s.Nc;
+    const float2 x1 = x_at<REAL, POW2>(s, Zb, kk);
+    const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
+    const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
+    if (owner) {
+      store_ext<REAL>(s.X + (size_t)b * a.xs, s.N, a.maxn, kk, x1);
+      const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
+      acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
     }
-    if (owner) a.acc[kk] = acc;
+    if (++cnt >= a.averages) {
+      if (owner) emit_record(a, r, kk, acc, cnt);
+      acc = 0.0f;
+      cnt = 0;
+      ++r;
+    }
   }
-  if (a.trace) {
-    __syncthreads();
-    trace_end(a.trace, 2);
-  }
+  if (owner) a.acc[kk] = acc;
+  trace_end(a.trace, 2);
 }
 
 // ----------------------------------------------------------------- filter bank
@@ -535,10 +653,7 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       if (threadIdx.x == 0) next = atomicAdd(a.cursor, 1);
     } else {
       if (it) {
-        if (a.trace) {
-          __syncthreads();
-          trace_end(a.trace, 3);
-        }
+        trace_end(a.trace, 3);
         return;
       }
       tile = tile_base + blockIdx.x;
@@ -551,7 +666,7 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
       const int logp = CHIRP ? 0 : max(0, td.log2n - ilog2c(S));   // split into 2^logp parts: entry (channel, P block + part)
       const int b = cb.y >> logp;
       TileMeta m;
-      m.X = a.X + (size_t)b * a.xs + (ch.first & ((1ll << a.log2N) - 1));
+      m.X = a.X + (size_t)b * a.xs + ch.first;                // first is already modulo N
       m.w = ch.w;
       m.out = ch.out + (size_t)b * keep;
       m.pad = cb.y & ((1 << logp) - 1);
@@ -567,51 +682,110 @@ __global__ void __launch_bounds__(T, MINB) fcfb_kernel(FcfbArgs a, int tile_base
   }
 }
 
-// Adjoint of fcfb_kernel.  With g = FFT_n(dy zero-padded to [n/8, 7n/8)) (the
-// forward transform is the adjoint of the unnormalised inverse), v = w * G:
-//   dW[j] += conj(G[j]) g,  dX[bin] += conj(w[j]) g  (conjugated for mirror bins).
-template <int S, int T, bool REAL>
-__global__ void __launch_bounds__(T, 2) fcfb_backward_kernel(BwdArgs a) {
+// Adjoint of fcfb_kernel, deterministic (no atomics: every sum runs in a
+// fixed order, so two runs give the same bits).  With g = FFT_n(dy zero-padded
+// to [n/8, 7n/8)) (the forward transform is the adjoint of the unnormalised
+// inverse) and v = w * G, G = get_bin(X, first + j):
+//   dW[j] = sum over blocks, in block order, of conj(G[j]) g[j]
+//   dX[bin] += sum over the (channel, j) that gather the bin, in channel
+//              order, of conj(w[j]) g[j] (conjugated for mirror bins).
+// Step 1: g of every (channel, block) transform on the staged tile pipeline
+// (forward FFT, load = padded dy, store = the channel's g scratch).
+struct BwdMeta {
+  const float2* dy;     // block's output gradients, 6(n/8)
+  float2* g;            // block's row of the channel's g scratch, n, indexed by weight index j
+};
+
+template <int LOGN, int S, int T>
+__device__ __forceinline__ void bwd_tile(float2* sm, const BwdMeta* meta, int count, const float2* tw) {
+  constexpr int n = 1 << LOGN, lo = n >> 3, keep = 6 * lo;
+  using P = StagePlan<LOGN, S / T>;
+  auto load = [&](int t, int q, int s) {
+    const int i = q + (s << P::first_shift) - lo;
+    if constexpr (keep == 0) return make_float2(0.f, 0.f);  // n = 4 keeps no outputs
+    else return (unsigned)i < (unsigned)keep ? __ldg(&meta[t].dy[i]) : make_float2(0.f, 0.f);
+  };
+  // FFT output o pairs with IFFT input o, whose weight index is j = (o + n/2) mod n
+  // (fcfb.rs:166-169): g is stored by j, so g[j] multiplies conj(G[j]) and conj(w[j]).
+  auto store = [&](int t, int q, int u, float2 v) {
+    meta[t].g[(q + (u << P::last_shift) + n / 2) & (n - 1)] = v;
+  };
+  tile_pipeline<LOGN, S, T, -1, true>(sm, count, tw, load, store);
+}
+
+template <int S, int T>
+__global__ void __launch_bounds__(T, 2) fcfb_bwd_fft_kernel(BwdArgs a) {
   extern __shared__ float2 sm[];
-  constexpr int E = S / T;
-  const int N = 1 << a.log2N;
+  __shared__ BwdMeta s_meta[MAX_TILE_TRANSFORMS];
+  static_assert(MAX_TILE_TRANSFORMS <= T, "one thread stages one transform's metadata");
   const TileDesc td = a.tiles[blockIdx.x];
-  const int log2n = td.log2n, n = 1 << log2n, half = n >> 1;
-  const int lo = n >> 3, keep = 6 * lo;
-  for (int k = 0; k < E; ++k) {
-    const int e = threadIdx.x + k * T;
-    const int t = e >> log2n, i = e & (n - 1);
-    float2 v = make_float2(0.f, 0.f);
-    if (t < td.count && i >= lo && i < lo + keep) {
-      const int2 cb = a.list[td.list_off + t];
-      v = a.chans[cb.x].dy[(size_t)cb.y * keep + (i - lo)];
-    }
-    sm[padx(e)] = v;
+  if (threadIdx.x < td.count) {
+    const int2 cb = __ldg(&a.list[td.list_off + threadIdx.x]);
+    const BwdChan& ch = a.chans[cb.x];
+    const int n = 1 << td.log2n;
+    s_meta[threadIdx.x] = BwdMeta{ch.dy + (size_t)cb.y * (6 * (n >> 3)), ch.g + (size_t)cb.y * n};
   }
   __syncthreads();
-  tile_fft<-1, S, T>(sm, a.tw, log2n);
-  for (int k = 0; k < E; ++k) {
-    const int e = threadIdx.x + k * T;
-    const int t = e >> log2n, i = e & (n - 1);
-    if (t >= td.count) continue;
-    const int2 cb = a.list[td.list_off + t];
-    const BwdChan& ch = a.chans[cb.x];
-    const float2 g = sm[padx(e)];
-    const int j = (i + half) & (n - 1);
-    const int m = (int)((ch.first + j) & (long long)(N - 1));
-    const bool mirror = REAL && m >= a.K;
-    const size_t xi = (size_t)cb.y * a.K + (mirror ? N - m : m);
-    const float2 G = mirror ? cconj(a.X[xi]) : a.X[xi];
-    const float2 dw = cmul(cconj(G), g);
-    atomicAdd(&ch.dw[j].x, dw.x);
-    atomicAdd(&ch.dw[j].y, dw.y);
-    if (a.dX) {
-      float2 dg = cmul(cconj(ch.w[j]), g);
-      if (mirror) dg = cconj(dg);
-      atomicAdd(&a.dX[xi].x, dg.x);
-      atomicAdd(&a.dX[xi].y, dg.y);
-    }
+  switch (td.log2n) {
+    case 2: bwd_tile<2, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 3: bwd_tile<3, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 4: bwd_tile<4, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 5: bwd_tile<5, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 6: bwd_tile<6, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 7: bwd_tile<7, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 8: bwd_tile<8, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 9: bwd_tile<9, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 10: bwd_tile<10, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 11: bwd_tile<11, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 12: bwd_tile<12, S, T>(sm, s_meta, td.count, a.tw); break;
+    case 13: bwd_tile<13, S, T>(sm, s_meta, td.count, a.tw); break;
   }
+}
+
+// get_bin on the [B][K] spectra: bin (first + j) mod N of block b, and
+// whether it is the conjugate mirror (real input, m >= K).
+template <bool REAL>
+__device__ __forceinline__ float2 bwd_bin(const BwdArgs& a, int b, long long first, int j) {
+  const int m = (int)((first + j) % a.N);
+  const bool mirror = REAL && m >= a.K;
+  const float2 x = __ldg(&a.X[(size_t)b * a.K + (mirror ? a.N - m : m)]);
+  return mirror ? cconj(x) : x;
+}
+
+// Step 2: dW[c][j] = sum_b conj(G_b[j]) g_b[j], one thread per (channel, j).
+template <bool REAL>
+__global__ void __launch_bounds__(256) fcfb_bwd_dw_kernel(BwdArgs a) {
+  const int c = blockIdx.y, j = blockIdx.x * 256 + threadIdx.x;
+  const BwdChan& ch = a.chans[c];
+  const int n = 1 << ch.log2n;
+  if (j >= n) return;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int b = 0; b < a.B; ++b) {
+    const float2 G = bwd_bin<REAL>(a, b, ch.first, j);
+    acc = cadd(acc, cmul(cconj(G), __ldg(&ch.g[(size_t)b * n + j])));
+  }
+  ch.dw[j] = acc;
+}
+
+// Step 3: dX[b][k] += sum over bin k's gather list (channel order) of
+// conj(w[j]) g_b[j], conjugated for mirror entries; one thread per (b, k).
+template <int V = 0>   // a template, so that every translation unit including this header shares one instance
+__global__ void __launch_bounds__(256) fcfb_bwd_dx_kernel(BwdArgs a) {
+  const int b = blockIdx.y, k = blockIdx.x * 256 + threadIdx.x;
+  if (k >= a.K) return;
+  float2 acc = make_float2(0.f, 0.f);
+  const int e1 = __ldg(&a.bin_off[k + 1]);
+  for (int e = __ldg(&a.bin_off[k]); e < e1; ++e) {
+    const int2 ent = __ldg(&a.bin_ent[e]);
+    const BwdChan& ch = a.chans[ent.x];
+    const int j = ent.y >> 1;
+    const int n = 1 << ch.log2n;
+    float2 d = cmul(cconj(__ldg(&ch.w[j])), __ldg(&ch.g[(size_t)b * n + j]));
+    if (ent.y & 1) d = cconj(d);
+    acc = cadd(acc, d);
+  }
+  float2* x = a.dX + (size_t)b * a.K + k;
+  *x = cadd(*x, acc);
 }
 
 }  // namespace sk

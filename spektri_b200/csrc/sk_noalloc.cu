@@ -178,6 +178,9 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   a.B = (int)n_blocks;
   a.log2N = log2N;
   a.log2Nc = log2Nc;
+  a.N = (int)N;
+  a.Nc = (int)Nc;
+  a.logM = TILE_LOGS;
   a.R1 = 1;
   a.log2R1 = 0;
   if (log2Nc > TILE_LOGS) {
@@ -202,12 +205,12 @@ extern "C" int sk_spectra_noalloc(const void* raw, int32_t input_format, uint32_
   s.Z = Z;
   s.X = (float2*)X;
   s.P = nullptr;
-  s.log2N = log2N;
-  s.log2Nc = log2Nc;
+  s.N = (int)N;
+  s.Nc = (int)Nc;
   s.K = cplx ? (int)N : (int)(N / 2 + 1);
   s.R1 = a.R1;
   s.log2R1 = a.log2R1;
-  s.logS = TILE_LOGS;
+  s.logM = TILE_LOGS;
   s.tw_big = tw_big;
   e = launch_split(cplx, (int)n_blocks, s, st);
   if (e != cudaSuccess) return fail(SK_ERR_CUDA, "spectrum split kernel: %s", cudaGetErrorString(e));

@@ -67,7 +67,9 @@ struct sk_plan {
   bool cplx = false;
   long long N = 0, overlap = 0, hop = 0, nnew = 0, total = 0;
   int K = 0, B = 0;
-  int log2N = 0, log2Nc = 0, R1 = 1, log2R1 = 0;
+  int log2N = 0, log2Nc = 0, R1 = 1, log2R1 = 0;   // log2N, log2Nc = -1 and log2R1 = -1 for mixed-radix sizes
+  long long Nc = 0;                     // complex FFT length (N/2 real, N complex)
+  int logM = TILE_LOGS;                 // two-pass forward FFT: row length M = Nc / R1
   int fwd_per = 1;                      // single-pass forward FFT (Nc <= 8192): blocks per tile
   float wscale = 0.f;
   int spec_fmt = 0, spec_bin_bytes = 1;
@@ -114,6 +116,9 @@ struct sk_plan {
   std::vector<ChanDev> h_chans_uploaded;
   ChanDev* d_chans_aux = nullptr;
   BwdChan* d_bwd = nullptr;
+  float2* d_bwd_g = nullptr;            // adjoint scratch: per channel B * n (allocated by the first adjoint call)
+  int* d_bin_off = nullptr;             // adjoint dX gather lists per spectrum bin
+  int2* d_bin_ent = nullptr;
   struct TileSet {                      // filter-bank work list for one tile size
     int size = 0;
     TileDesc* d_tiles = nullptr;        // batched tiles first, then each channel's own (plain mode)
@@ -163,7 +168,7 @@ int plan_free(sk_plan* pl) {
   void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_tw_split, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->ts[0].d_tiles, pl->ts[0].d_list,
                   pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec,
-                  pl->d_blu, pl->d_blu_tab, pl->d_trace};
+                  pl->d_blu, pl->d_blu_tab, pl->d_trace, pl->d_bwd_g, pl->d_bin_off, pl->d_bin_ent};
   if (pl->h_trace) cudaFreeHost(pl->h_trace);
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
   if (pl->graph) cudaGraphDestroy(pl->graph);
@@ -175,6 +180,8 @@ int plan_free(sk_plan* pl) {
   delete pl;
   return SK_OK;
 }
+
+#define TRY_NOFREE(x) do { const int rc_ = (x); if (rc_ != SK_OK) return rc_; } while (0)
 
 template <class TT>
 int dev_alloc(TT** p, size_t count) {
@@ -247,8 +254,11 @@ FwdArgs fwd_args(const sk_plan* pl, const uint8_t* raw) {
   a.B = pl->B;
   a.log2N = pl->log2N;
   a.log2Nc = pl->log2Nc;
+  a.N = (int)pl->N;
+  a.Nc = (int)pl->Nc;
   a.R1 = pl->R1;
   a.log2R1 = pl->log2R1;
+  a.logM = pl->logM;
   a.wscale = pl->wscale;
   a.tw_tile = pl->d_tw_tile;
   a.tw_big = pl->d_tw_big;
@@ -271,12 +281,12 @@ SplitArgs split_args(const sk_plan* pl, float2* X) {
   s.Z = pl->d_Z;
   s.X = X;
   s.P = nullptr;
-  s.log2N = pl->log2N;
-  s.log2Nc = pl->log2Nc;
+  s.N = (int)pl->N;
+  s.Nc = (int)pl->Nc;
   s.K = pl->K;
   s.R1 = pl->R1;
   s.log2R1 = pl->log2R1;
-  s.logS = TILE_LOGS;
+  s.logM = pl->logM;
   s.tw_big = pl->d_tw_big;
   return s;
 }
@@ -300,7 +310,13 @@ WelchArgs welch_args(const sk_plan* pl, float2* X, const WelchCall& c) {
 // The forward FFT kernel(s): one kernel for Nc <= 8192 (whole blocks per
 // tile), else the column pass into d_Y (registers for R1 <= 8, shared memory
 // above) followed by the row pass into d_Z.
-int fwd_kind(const sk_plan* pl) { return pl->R1 == 1 ? 0 : pl->R1 > 8 ? 1 : 2; }
+int fwd_kind(const sk_plan* pl) { return pl->R1 == 1 ? 0 : pl->log2R1 < 0 ? 3 : pl->R1 > 8 ? 1 : 2; }
+
+// Row-pass tiles: 8192 / M rows of M points each.
+int rows_grid(const sk_plan* pl) {
+  const int rpt = S >> pl->logM;
+  return (pl->B * pl->R1 + rpt - 1) / rpt;
+}
 
 // pdl: the row pass (if any) is launched as a programmatic dependent of the
 // column pass.
@@ -308,7 +324,7 @@ cudaError_t launch_fwd_any(const sk_plan* pl, const FwdArgs& a, cudaStream_t st,
   if (pl->R1 == 1) return launch_fwd(pl->fmt, fwd_grid(pl), a, st);
   const cudaError_t e = launch_fwd_col(pl->fmt, fwd_grid(pl), a, pl->d_Y, st);
   if (e != cudaSuccess) return e;
-  return launch_fwd_rows(fwd_grid(pl), a, pl->d_Y, st, pdl);
+  return launch_fwd_rows(rows_grid(pl), a, pl->d_Y, st, pdl);
 }
 
 int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* welch, cudaStream_t st,
@@ -472,8 +488,8 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     cudaGraphGetNodes(g, nullptr, &n);
     std::vector<cudaGraphNode_t> nodes(n);
     cudaGraphGetNodes(g, nodes.data(), &n);
-    const void* f_fwd = fwd_kernel_ptr(pl->fmt, fwd_kind(pl));
-    const void* f_welch = welch_kernel_ptr(pl->cplx, pl->B);
+    const void* f_fwd = fwd_kernel_ptr(pl->fmt, fwd_kind(pl), pl->R1);
+    const void* f_welch = welch_kernel_ptr(pl->cplx, pl->B, pl->log2N >= 0);
     for (auto nd : nodes) {
       cudaGraphNodeType t;
       if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
@@ -533,11 +549,31 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   if (p.ffts_per_buf == 0) return fail(SK_ERR_ARG, "fftbuf must be positive");
   const bool cplx = format_complex(p.input_format);
   if (!cplx && (p.ffts_per_buf % 2)) return fail(SK_ERR_ARG, "fftbuf must be even for real input (blocks are transformed in pairs, multifft.rs:57-61)");
-  const int log2N = ilog2_exact(p.fft_size);
-  const int log2Nc = log2N - (cplx ? 0 : 1);
-  if (log2N < 0 || log2Nc < 2 || log2N < 3) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path needs a power of two >= 8", p.fft_size);
-  const int maxLogNc = TILE_LOGS + 8;   // R1 <= 256
-  if (log2Nc > maxLogNc) return fail(SK_ERR_UNSUPPORTED, "FFT size %u exceeds the device limit (complex length %d)", p.fft_size, 1 << maxLogNc);
+  // Forward FFT sizes (multifft.rs:25-30 plans any size): powers of two with
+  // Nc = N/2 (real) or N (complex) from 4 to 2^21, and Nc = R1 * M with
+  // R1 = 3, 5, 6, 10, 12 and M a power of two from 16 to 8192 (the
+  // mixed-radix column pass; N = 3 * 2^k and 5 * 2^k, e.g. 12288, 49152, 98304).
+  int log2N = ilog2_exact(p.fft_size);
+  int log2Nc = log2N < 0 ? -1 : log2N - (cplx ? 0 : 1);
+  const long long Nc = cplx ? (long long)p.fft_size : (long long)p.fft_size / 2;
+  int mixR1 = 0, mixLogM = 0;
+  if (log2N < 0) {
+    if (!cplx && (p.fft_size % 2)) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: odd sizes of real input are not supported on the device", p.fft_size);
+    for (int r0 : {3, 5})
+      for (int pw = 1; pw <= 4 && !mixR1; pw *= 2) {
+        const long long r1 = (long long)r0 * pw;
+        if (!mixed_r1_ok((int)r1) || Nc % r1) continue;
+        const int lm = ilog2_exact(Nc / r1);
+        if (lm >= 4 && lm <= TILE_LOGS) { mixR1 = (int)r1; mixLogM = lm; }
+      }
+    if (!mixR1)
+      return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path takes powers of two and 3 * 2^k or 5 * 2^k with "
+                  "the complex length up to 12 * 8192", p.fft_size);
+  } else {
+    if (log2Nc < 2 || log2N < 3) return fail(SK_ERR_UNSUPPORTED, "FFT size %u: the device path needs a power of two >= 8", p.fft_size);
+    const int maxLogNc = TILE_LOGS + 8;   // R1 <= 256
+    if (log2Nc > maxLogNc) return fail(SK_ERR_UNSUPPORTED, "FFT size %u exceeds the device limit (complex length %d)", p.fft_size, 1 << maxLogNc);
+  }
 
   sk_plan* pl = new sk_plan();
   pl->p = p;
@@ -552,7 +588,12 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   pl->K = cplx ? (int)pl->N : (int)(pl->N / 2 + 1);
   pl->log2N = log2N;
   pl->log2Nc = log2Nc;
-  if (log2Nc > TILE_LOGS) {
+  pl->Nc = Nc;
+  if (mixR1) {
+    pl->R1 = mixR1;
+    pl->log2R1 = -1;
+    pl->logM = mixLogM;
+  } else if (log2Nc > TILE_LOGS) {
     pl->log2R1 = log2Nc - TILE_LOGS;
     pl->R1 = 1 << pl->log2R1;
   }
@@ -637,8 +678,8 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
   const size_t halo_n = (size_t)pl->overlap * (cplx ? 2 : 1);
   TRY(dev_alloc(&pl->d_halo[0], halo_n));
   TRY(dev_alloc(&pl->d_halo[1], halo_n));
-  TRY(dev_alloc(&pl->d_Z, (size_t)pl->B << pl->log2Nc));
-  if (pl->R1 > 1) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B << pl->log2Nc));
+  TRY(dev_alloc(&pl->d_Z, (size_t)pl->B * pl->Nc));
+  if (pl->R1 > 1) TRY(dev_alloc(&pl->d_Y, (size_t)pl->B * pl->Nc));
   TRY(dev_alloc(&pl->d_X, (size_t)pl->B * pl->xs));
   TRY(dev_alloc(&pl->d_acc, (size_t)pl->K));
   TRY(dev_alloc(&pl->d_w, pl->w_host.size() / 2));
@@ -697,7 +738,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     ChanDev d{};
     d.w = pl->d_w + pl->ch[c].w_off;
     d.out = pl->d_out + pl->ch[c].out_off;
-    d.first = pl->ch[c].first;
+    d.first = ((pl->ch[c].first % pl->N) + pl->N) % pl->N;   // the kernels take first modulo N
     d.log2n = pl->ch[c].log2n;
     pl->h_chans[c] = d;
     pl->d_out_ptrs.push_back(d.out);
@@ -1049,7 +1090,7 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   }
   if (pl->ch.empty()) return SK_OK;
   // The caller's [B][K] spectra into the plan's extended rows, then the filter bank.
-  SK_CUDA(launch_extend(pl->cplx, pl->B, (const float2*)X, pl->K, pl->log2N, pl->d_X, pl->xs, pl->maxn, st));
+  SK_CUDA(launch_extend(pl->cplx, pl->B, (const float2*)X, pl->K, (int)pl->N, pl->d_X, pl->xs, pl->maxn, st));
   FcfbArgs a = fcfb_args(pl, pl->d_chans_aux, pl->d_X);
   const sk_plan::TileSet& t = cur_tiles(pl);
   if (t.n_chirp > 0) SK_CUDA(launch_fcfb(false, true, pl->fcfb_size, pl->fcfb_threads, t.n_chirp, a, 0, st));
@@ -1069,31 +1110,69 @@ int sk_fcfb_backward_device(sk_plan* pl, const float* X, const float* const* W, 
   for (const auto& c : pl->ch)
     if (c.log2n > TILE_LOGS)
       return fail(SK_ERR_UNSUPPORTED, "the adjoint covers IFFT sizes up to %d; this plan has one of %u", TILE_S, c.n);
+  if (pl->ch.empty()) return SK_OK;
   DeviceGuard g(pl->p.device);
   cudaStream_t st = stream ? (cudaStream_t)stream : pl->stream;
+  if (!pl->d_bwd_g) {
+    // First adjoint call: the g scratch (B * n per channel) and, per spectrum
+    // bin, the list of (channel, j) that gather it, in channel then j order.
+    size_t total = 0;
+    std::vector<int> cnt((size_t)pl->K + 1, 0);
+    auto bin_of = [&](const sk_plan::Chan& c, int j, bool* mirror) {
+      const long long m = (((c.first % pl->N) + pl->N) % pl->N + j) % pl->N;
+      *mirror = !pl->cplx && m >= pl->K;
+      return (int)(*mirror ? pl->N - m : m);
+    };
+    bool mir = false;
+    for (const auto& c : pl->ch) {
+      total += (size_t)pl->B * c.n;
+      for (uint32_t j = 0; j < c.n; ++j) cnt[bin_of(c, (int)j, &mir)]++;
+    }
+    std::vector<int> off((size_t)pl->K + 1, 0);
+    for (int k = 0; k < pl->K; ++k) off[k + 1] = off[k] + cnt[k];
+    std::vector<int2> ent((size_t)off[pl->K]);
+    std::vector<int> pos(off.begin(), off.end() - 1);
+    for (size_t ci = 0; ci < pl->ch.size(); ++ci)
+      for (uint32_t j = 0; j < pl->ch[ci].n; ++j) {
+        const int k = bin_of(pl->ch[ci], (int)j, &mir);
+        ent[pos[k]++] = make_int2((int)ci, 2 * (int)j + (mir ? 1 : 0));
+      }
+    TRY_NOFREE(dev_alloc(&pl->d_bwd_g, total));
+    TRY_NOFREE(dev_alloc(&pl->d_bin_off, off.size()));
+    TRY_NOFREE(dev_alloc(&pl->d_bin_ent, ent.size()));
+    SK_CUDA(cudaMemcpy(pl->d_bin_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    if (!ent.empty()) SK_CUDA(cudaMemcpy(pl->d_bin_ent, ent.data(), sizeof(int2) * ent.size(), cudaMemcpyHostToDevice));
+  }
   std::vector<BwdChan> bc(pl->ch.size());
+  size_t goff = 0;
+  int max_n = 0;
   for (size_t c = 0; c < bc.size(); ++c) {
     if (!W[c] || !dy[c] || !dW[c]) return fail(SK_ERR_ARG, "null pointer for channel %zu", c);
     bc[c].w = (const float2*)W[c];
     bc[c].dy = (const float2*)dy[c];
     bc[c].dw = (float2*)dW[c];
-    bc[c].first = pl->ch[c].first;
+    bc[c].g = pl->d_bwd_g + goff;
+    goff += (size_t)pl->B * pl->ch[c].n;
+    bc[c].first = ((pl->ch[c].first % pl->N) + pl->N) % pl->N;
     bc[c].log2n = pl->ch[c].log2n;
-    SK_CUDA(cudaMemsetAsync(dW[c], 0, sizeof(float2) * pl->ch[c].n, st));
+    max_n = std::max(max_n, (int)pl->ch[c].n);
   }
-  if (bc.empty()) return SK_OK;
   SK_CUDA(cudaMemcpyAsync(pl->d_bwd, bc.data(), sizeof(BwdChan) * bc.size(), cudaMemcpyHostToDevice, st));
   SK_CUDA(cudaStreamSynchronize(st));
   BwdArgs a{};
-  a.tiles = pl->ts[0].d_tiles;          // the adjoint runs on 8192-point tiles
+  a.tiles = pl->ts[0].d_tiles;          // the adjoint's FFTs run on 8192-point tiles
   a.list = pl->ts[0].d_list;
   a.chans = pl->d_bwd;
+  a.nchan = (int)pl->ch.size();
   a.X = (const float2*)X;
   a.dX = (float2*)dX;
+  a.bin_off = pl->d_bin_off;
+  a.bin_ent = pl->d_bin_ent;
   a.K = pl->K;
-  a.log2N = pl->log2N;
+  a.N = (int)pl->N;
+  a.B = pl->B;
   a.tw = pl->d_tw_tile;
-  SK_CUDA(launch_fcfb_backward(pl->cplx, pl->ts[0].n_batched, a, st));
+  SK_CUDA(launch_fcfb_backward(pl->cplx, pl->ts[0].n_batched, max_n, a, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }

@@ -34,15 +34,16 @@ constexpr int WELCH_CHUNK = 64;           // blocks whose Welch terms a CTA stag
 struct ChanDev {               // one filter-bank channel, as the kernels see it
   const float2* w;             // weights, natural order: w[j] scales bin first+j
   float2* out;                 // B * 6(n/8) outputs
-  long long first;
+  long long first;             // first bin modulo N (in [0, N))
   int log2n;
   int pad;
 };
 struct BwdChan {
   const float2* w;
   const float2* dy;            // B * 6(n/8) output gradients
-  float2* dw;                  // n weight gradients (accumulated)
-  long long first;
+  float2* dw;                  // n weight gradients (written)
+  float2* g;                   // scratch, B * n: per block the forward FFT of dy zero-padded to [n/8, 7n/8)
+  long long first;             // first bin modulo N
   int log2n;
   int pad;
 };
@@ -77,8 +78,11 @@ struct FwdArgs {
   float* halo_next;            // receives the converted last N/4 samples of this one
   long long overlap, nnew;
   int hop, B;
-  int log2N, log2Nc;           // N (window length) and Nc (complex FFT length)
-  int R1, log2R1;              // Nc = R1 * S when Nc > S (R1 = 1 otherwise)
+  int log2N, log2Nc;           // N (window length) and Nc (complex FFT length), powers of two (else -1)
+  int N, Nc;                   // the same lengths (any supported size)
+  int R1, log2R1;              // two-pass FFTs: Nc = R1 * M (R1 = 1: single pass); log2R1 = -1 when R1
+                               // is not a power of two (R1 = 3, 5, 6, 10, 12: the mixed-radix column pass)
+  int logM;                    // two-pass FFTs: log2 of the row length M (8192 when R1 is a power of two)
   float wscale;                // rectangular window value scaling/N (dsp.rs:70-73)
   const float2* tw_tile;       // W_S^k
   const float2* tw_big;        // W_N^k, k < N
@@ -90,10 +94,10 @@ struct FwdArgs {
 };
 
 struct SplitArgs {
-  const float2* Z;
+  const float2* Z;             // [B][Nc] packed spectra; residue layout for R1 > 1 (k1 + R1 k2 at k1 M + k2)
   float2* X;                   // [B][K]
   float* P;                    // [B][K] Welch terms (may be null)
-  int log2N, log2Nc, K, R1, log2R1, logS;
+  int N, Nc, K, R1, log2R1, logM;   // log2R1 = -1: R1 not a power of two
   const float2* tw_big;        // W_N^k
 };
 
@@ -125,12 +129,15 @@ struct FcfbArgs {
 };
 
 struct BwdArgs {
-  const TileDesc* tiles;
-  const int2* list;
+  const TileDesc* tiles;       // the 8192-point tiles of the plan (power-of-two sizes <= 8192)
+  const int2* list;            // (channel, block) per transform
   const BwdChan* chans;
-  const float2* X;
-  float2* dX;                  // may be null
-  int K, log2N;
+  int nchan;
+  const float2* X;             // [B][K] spectra of the forward pass
+  float2* dX;                  // [B][K], accumulated into (may be null)
+  const int* bin_off;          // dX gather lists: bin k's entries are bin_ent[bin_off[k] .. bin_off[k+1])
+  const int2* bin_ent;         // (channel, 2 j + mirror): get_bin(first + j) is bin k (conjugated if mirror)
+  int K, N, B;
   const float2* tw;
 };
 
@@ -158,7 +165,7 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
 cudaError_t launch_split(bool cplx, int B, const SplitArgs& s, cudaStream_t st);
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl = false);
 // [B][K] spectra (the differentiable stage's layout) -> [B][xs] extended rows.
-cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int log2N, float2* Xe, long long xs, int maxn,
+cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int N, float2* Xe, long long xs, int maxn,
                           cudaStream_t st);
 cudaError_t fcfb_prepare();
 // Filter-bank tile shapes (tile_size, tile_threads): (8192, 256), (8192, 512)
@@ -177,14 +184,19 @@ const void* fcfb_ptr_8192x512(bool persistent);
 const void* fcfb_ptr_8192x512_chirp(bool persistent);
 const void* fcfb_ptr_4096(bool persistent);
 const void* fcfb_ptr_4096_chirp(bool persistent);
-cudaError_t launch_fcfb_backward(bool cplx, int grid, const BwdArgs& a, cudaStream_t st);
+// Adjoint in three deterministic launches: the per-transform forward FFTs of
+// the padded output gradients (grid = tiles), dW summed over blocks in block
+// order (grid = channels x n_max/256), dX gathered per bin in channel order.
+cudaError_t launch_fcfb_backward(bool cplx, int grid, int max_n, const BwdArgs& a, cudaStream_t st);
 // Kernel entry addresses (to recognise the nodes of a captured graph).
 // kind 0: single-pass forward kernel; 1: shared-memory column pass (R1 >= 16);
-// 2: register column pass (R1 = 2..8).
-const void* fwd_kernel_ptr(int fmt, int kind);
-const void* fwd_kernel_ptr_8(int fmt, int kind);
-const void* fwd_kernel_ptr_16(int fmt, int kind);
-const void* fwd_kernel_ptr_32(int fmt, int kind);
-const void* welch_kernel_ptr(bool cplx, int B);
+// 2: register column pass (R1 = 2..8); 3: mixed-radix column pass (R1 = 3, 5, 6, 10, 12).
+const void* fwd_kernel_ptr(int fmt, int kind, int R1);
+const void* fwd_kernel_ptr_8(int fmt, int kind, int R1);
+const void* fwd_kernel_ptr_16(int fmt, int kind, int R1);
+const void* fwd_kernel_ptr_32(int fmt, int kind, int R1);
+// Mixed-radix column factors: R1 = R0 * P with R0 = 3 or 5 and P a power of two.
+constexpr bool mixed_r1_ok(int r1) { return r1 == 3 || r1 == 5 || r1 == 6 || r1 == 10 || r1 == 12; }
+const void* welch_kernel_ptr(bool cplx, int B, bool pow2);   // pow2: the FFT size is a power of two
 
 }  // namespace sk

@@ -14,6 +14,9 @@ Fixtures:
                          Python model of the filter bank, imported and run here) on
                          seeded int16 streams, real and complex, for several channels
   wire_topics.json       topic / metadata bytes from tools/spektri.py:15-42
+  ddc_ref.npz            outputs of tools/ddc.py:51-177 (RationalDdc designed by
+                         DesignDdc, imported and run here; needs numba and scipy)
+                         on seeded complex streams fed in uneven chunks
 """
 import importlib.util
 import json
@@ -126,6 +129,44 @@ def wire_topics():
             "metadata_hex": msg[:24].hex(), "metadata": [md.seq, md.time_s, md.time_ns]}
 
 
+DDC_CASES = [                      # (fs_in, fs_out, fc, samples)
+    (256000, 48000, 12000, 6000),
+    (64000, 16000, -3000, 4000),
+    (500000, 16000, 500, 12000),
+]
+
+
+def ddc_ref():
+    """RationalDdc outputs of the reference (tools/ddc.py) on seeded input,
+    fed in chunks of uneven size (the state carries across calls); the
+    reference's output buffer holds 1000 samples per call (ddc.py:105), so
+    chunks stay below 1000 * decimation / interpolation input samples."""
+    ddc = load_module(os.path.join(REF, "tools/ddc.py"), "ref_ddc")
+    out = {}
+    rng = np.random.default_rng(2024)
+    for i, (fs_in, fs_out, fc, n) in enumerate(DDC_CASES):
+        d = ddc.DesignDdc(fs_in, fs_out, fc)
+        x = ((rng.standard_normal(n) + 1j * rng.standard_normal(n)) * 0.3).astype(np.complex64)
+        t = np.arange(n)
+        x += (0.5 * np.exp(2j * np.pi * (fc + 0.1 * fs_out) / fs_in * t)).astype(np.complex64)
+        limit = max(1, 1000 * d.decimation // d.interpolation - 1)
+        ys, pos, k = [], 0, 0
+        while pos < n:
+            c = min(n - pos, min(limit, [517, 1999, 64, 3001, 1][k % 5]))
+            ys.append(d.execute(x[pos:pos + c]))
+            pos += c
+            k += 1
+        y = np.concatenate(ys)
+        from fractions import Fraction
+        f = -Fraction(fc) / Fraction(fs_in)
+        out[f"in{i}"] = x
+        out[f"taps{i}"] = np.asarray(d.taps, np.float32)
+        out[f"cfg{i}"] = np.array([d.interpolation, d.decimation, f.numerator, f.denominator, fs_in, fs_out, fc],
+                                  np.int64)
+        out[f"out{i}"] = y
+    np.savez_compressed(os.path.join(OUT, "ddc_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     if not REF or not os.path.isdir(os.path.join(REF, "spektri")):
         sys.exit("usage: make_golden.py <reference root>  (or set SPEKTRI_REFERENCE): the tejeez/spektri tree")
@@ -136,4 +177,5 @@ if __name__ == "__main__":
     with open(os.path.join(OUT, "wire_topics.json"), "w") as f:
         json.dump(wire_topics(), f, indent=1)
     proto_fcfb()
+    ddc_ref()
     print("golden fixtures written to", OUT)

@@ -186,3 +186,52 @@ def test_host_binary_streams_c3(tmp_path):
     per_buf = (times[20] - times[4]) / 16
     print(f"host binary, C3: {w.samples_per_buffer / per_buf / 1e6:.1f} Msamples/s "
           f"({per_buf * 1e3:.2f} ms per buffer of {w.samples_per_buffer} samples)")
+
+
+def test_sweep_through_host_binary(tmp_path):
+    """The reference's integration stimulus (test/test_spectrum.sh:7-16): the
+    testsignal sweep piped into the drop-in binary and into the oracle CLI.
+    Same record headers, u8 spectra within 1 LSB, channel records within
+    relative RMS 1e-5, and the spectral peak walks up the band record by
+    record as the sweep does (-pi to pi rad/sample over the run)."""
+    oracle32.build()
+    tsig = os.path.join(ROOT, "spektri_b200", "bin", "testsignal")
+    N, B, avg, n = 4096, 8, 8, 1 << 20
+    sig = subprocess.run([tsig, "-f", "cf32le", "-n", str(n)], capture_output=True, timeout=120, check=True).stdout
+    infile = tmp_path / "sweep.cf32"
+    infile.write_bytes(sig)
+    fs = 4.096e6
+    common = [f"--samplerate={fs:.17g}", "-n", str(N), "--fftbuf", str(B), f"--averages={avg}", "-I", "cf32le",
+              "--spectrumformat=u8", "--fake-clock=1700000000,1000000"]
+    env = dict(os.environ, SPEKTRI_LIBZMQ=libzmq_path() or "")
+
+    def run(binary, name):
+        d = tmp_path / name
+        d.mkdir()
+        f = d / "ch.bin"
+        args = [binary] + common + ["--zmqbind", f"ipc://{d}/sk.zmq", "--filters", f"fs=256000:fc=-1024000:file={f}"]
+        r = subprocess.run(args, stdin=open(infile, "rb"), capture_output=True, timeout=300, env=env)
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        return r.stdout, f.read_bytes()
+
+    out_o, ch_o = run(oracle32.CLI, "oracle")
+    out_h, ch_h = run(HOST, "host")
+    so, sh = split_records(out_o, N), split_records(out_h, N)
+    assert len(so) == len(sh) == (n // (3 * N // 4 * B)) * B // avg
+    peaks = []
+    for (ho, po), (hh, ph) in zip(so, sh):
+        assert ho == hh
+        a, b = np.frombuffer(po, np.uint8).astype(int), np.frombuffer(ph, np.uint8).astype(int)
+        assert np.max(np.abs(a - b)) <= 1
+        k = int(np.argmax(b))
+        peaks.append(k if k < N // 2 else k - N)               # signed bin: -N/2 .. N/2
+    steps = np.diff(np.array(peaks))
+    assert np.mean(steps > 0) > 0.9, peaks                     # the sweep rises through the band
+    keep = B * 256 // 8 * 6 * 8
+    ro, rh = split_records(ch_o, keep), split_records(ch_h, keep)
+    assert len(ro) == len(rh) and [h for h, _ in ro] == [h for h, _ in rh]
+    # over the whole run (the sweep crosses the channel once; elsewhere the
+    # channel holds only leakage, where both FP32 paths differ by rounding)
+    yo = np.concatenate([np.frombuffer(p, np.complex64) for _, p in ro])
+    yh = np.concatenate([np.frombuffer(p, np.complex64) for _, p in rh])
+    assert rel_rms(yh, yo) < 1e-5

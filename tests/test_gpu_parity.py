@@ -88,11 +88,16 @@ def test_all_formats_small(fmt):
 
 @pytest.mark.parametrize("fmt,N", [("s16le", 32768), ("s16le", 65536), ("cs16le", 4096),
                                    ("cs16le", 16384), ("cs16le", 65536), ("s16le", 8192), ("s16le", 16),
-                                   ("cs16le", 1 << 17), ("s16le", 1 << 18), ("cs16le", 1 << 20), ("s16le", 1 << 22)])
+                                   ("cs16le", 1 << 17), ("s16le", 1 << 18), ("cs16le", 1 << 20), ("s16le", 1 << 22),
+                                   ("s16le", 12288), ("s16le", 49152), ("s16le", 98304), ("cs16le", 12288),
+                                   ("cs16le", 49152), ("cs16le", 98304), ("s16le", 20480), ("cs16le", 81920),
+                                   ("cs16le", 48), ("s16le", 6144)])
 def test_fft_sizes_and_split_paths(fmt, N):
     """Single-tile FFTs, the fused residue split (Nc = R1 * 8192, R1 = 2..8),
     the two-pass column/row FFT (R1 = 16..256, up to 2^20 complex and 2^22
-    real points) and the smallest size."""
+    real points), the smallest size, and forward sizes 3 * 2^k and 5 * 2^k
+    (the reference takes any --fftsize, main.rs:43-44, multifft.rs:25-30):
+    a mixed-radix column pass (R1 = 3, 5, 6, 10, 12) and rows of M <= 8192."""
     rng = np.random.default_rng(N)
     B = 4 if N <= 1 << 17 else 2
     fs = float(N) * 1000.0
@@ -147,8 +152,12 @@ def test_edge_channels_wrap_mirror_and_drops():
 def test_invalid_parameters_rejected():
     with pytest.raises(SpektriError):
         Plan(1e6, 1024, "s16le", [], ffts_per_buf=3)          # odd fftbuf with real input
+    for N in (7 * 1024, 3 * 65536 * 2, 1000):                 # factor 7; complex length beyond 12 * 8192; 5^3
+        with pytest.raises(SpektriError) as e:
+            Plan(1e6, N, "cs16le", [], ffts_per_buf=2)
+        assert e.value.code == SK_ERR_UNSUPPORTED
     with pytest.raises(SpektriError):
-        Plan(1e6, 1000, "s16le", [], ffts_per_buf=2)          # not a power of two
+        Plan(1e6, 1000, "s16le", [], ffts_per_buf=2)          # 8 * 5^3: not a supported size
     with pytest.raises(SpektriError):
         Plan(1e6, 1 << 23, "s16le", [], ffts_per_buf=2)       # beyond 2^21 complex points
     p = Plan(1e6, 1024, "cs16le", [], ffts_per_buf=3)        # odd is fine for complex input
