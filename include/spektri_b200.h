@@ -167,7 +167,9 @@ int sk_get_weights(const sk_plan* plan, int32_t channel, float* weights_c64);
  *                payloads of the spectrum records completed by this call
  * sk_process takes host pointers (copies in, computes, copies out, returns
  * when done).  sk_process_device takes device pointers and only enqueues on
- * `stream` (a cudaStream_t; NULL = the plan's own stream). */
+ * `stream` (a cudaStream_t; NULL = the plan's own stream, which is non-blocking:
+ * work on the legacy default stream is not ordered with it, so a caller whose
+ * buffers belong to the legacy default stream passes cudaStreamLegacy). */
 int sk_process(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out, sk_result* result);
 int sk_process_device(sk_plan* plan, const void* raw, void* const* chan_out, void* spec_out,
                       sk_result* result, void* stream);

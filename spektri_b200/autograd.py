@@ -22,6 +22,13 @@ import torch
 from .plan import Plan
 
 
+def _plain(t: torch.Tensor) -> torch.Tensor:
+    """The tensor's values in plain contiguous memory: a lazily conjugated or
+    negated view (``y.conj()``, and the gradients that flow back through one)
+    keeps its data unconjugated with a flag, which a raw pointer would lose."""
+    return t.resolve_conj().resolve_neg().contiguous()
+
+
 def _zeros_for(plan, X):
     return [torch.zeros(c["out_samples"], dtype=torch.complex64, device=X.device) for c in plan.channels]
 
@@ -32,8 +39,8 @@ class FcfbFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, plan: Plan, X: torch.Tensor, *W: torch.Tensor):
         ys = [torch.empty(c["out_samples"], dtype=torch.complex64, device=X.device) for c in plan.channels]
-        Xc = X.contiguous()
-        Wc = [w.contiguous() for w in W]
+        Xc = _plain(X)
+        Wc = [_plain(w) for w in W]
         plan.fcfb_forward_device(Xc, Wc, ys, stream=torch.cuda.current_stream(X.device))
         ctx.plan = plan
         ctx.save_for_backward(Xc, *Wc)
@@ -44,7 +51,7 @@ class FcfbFunction(torch.autograd.Function):
         X, *W = ctx.saved_tensors
         plan = ctx.plan
         zeros = _zeros_for(plan, X)
-        dys = [z if d is None else d.contiguous() for z, d in zip(zeros, dys)]
+        dys = [z if d is None else _plain(d) for z, d in zip(zeros, dys)]
         dW = [torch.empty_like(w) for w in W]
         dX = torch.zeros_like(X) if ctx.needs_input_grad[1] else None
         plan.fcfb_backward_device(X, W, dys, dW, dX, stream=torch.cuda.current_stream(X.device))
@@ -59,7 +66,7 @@ class FcfbRecompute(torch.autograd.Function):
     def forward(ctx, plan: Plan, raw_window: torch.Tensor, *W: torch.Tensor):
         X = spectra_window(plan, raw_window)
         ys = [torch.empty(c["out_samples"], dtype=torch.complex64, device=raw_window.device) for c in plan.channels]
-        Wc = [w.contiguous() for w in W]
+        Wc = [_plain(w) for w in W]
         plan.fcfb_forward_device(X, Wc, ys, stream=torch.cuda.current_stream(raw_window.device))
         ctx.plan = plan
         ctx.save_for_backward(raw_window, *Wc)
@@ -71,7 +78,7 @@ class FcfbRecompute(torch.autograd.Function):
         plan = ctx.plan
         X = spectra_window(plan, raw_window)               # recomputed, bit-identical
         zeros = _zeros_for(plan, X)
-        dys = [z if d is None else d.contiguous() for z, d in zip(zeros, dys)]
+        dys = [z if d is None else _plain(d) for z, d in zip(zeros, dys)]
         dW = [torch.empty_like(w) for w in W]
         plan.fcfb_backward_device(X, W, dys, dW, None, stream=torch.cuda.current_stream(X.device))
         return (None, None, *dW)

@@ -192,11 +192,7 @@ class Plan:
     def process_device(self, raw, outs, spec, stream=None) -> _lib.Result:
         """Device path: torch CUDA tensors (or raw device pointers).  Enqueues
         on ``stream`` (torch stream / handle; default: torch's current stream)."""
-        if stream is None:
-            import torch
-            stream = torch.cuda.current_stream(self.device).cuda_stream
-        elif hasattr(stream, "cuda_stream"):
-            stream = stream.cuda_stream
+        stream = _stream(stream, self.device)
         r = _lib.Result()
         tbl = self._table([_ptr(o) for o in outs])
         check(lib().sk_process_device(self._h, _ptr(raw), tbl, _ptr(spec) if spec is not None else None,
@@ -286,8 +282,16 @@ class Plan:
                                             stream), "sk_fcfb_backward_device")
 
 
+CUDA_STREAM_LEGACY = 1        # cudaStreamLegacy: the legacy default stream, named explicitly
+
+
 def _stream(stream, device):
+    """The cudaStream_t handle for a torch stream (default: torch's current
+    stream) or a raw handle.  Torch's default stream has handle 0, which the
+    C ABI reads as "the plan's own stream" (non-blocking, unordered with
+    torch's work), so it is passed as cudaStreamLegacy instead."""
     if stream is None:
         import torch
-        return torch.cuda.current_stream(device).cuda_stream
-    return stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        stream = torch.cuda.current_stream(device)
+    h = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    return h if h else CUDA_STREAM_LEGACY
