@@ -391,39 +391,42 @@ __device__ __forceinline__ float2 rot_inv(float2 v, int k) {
 // same digit window as an S-point transform's, at P (k - S/8) + r.  The
 // twiddle e^{+2 pi i i r/n} is the conjugate of W_n^(i r) from the split
 // table (W_Ns^k, Ns the largest such n of the plan).
-template <int S, int T, int LOGP>
-__device__ __forceinline__ void fcfb_tile_part(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
+template <int S, int LOGP>
+__device__ __forceinline__ float2 part_input(const TileMeta& m, const FcfbTileConst& c, int i) {
   constexpr int LOGS = ilog2c(S), P = 1 << LOGP, LOGN = LOGS + LOGP;
-  using PL = StagePlan<LOGS, S / T>;
-  constexpr int RL = 1 << PL::last;
-  const TileMeta& m = meta[0];
   const int r = m.pad;
   // W_n^k: the tile table itself when n = 8192 (compile-time offsets), else
   // the split table at k << shn
   const float2* __restrict__ twn = LOGN == TILE_LOGS ? c.tw : c.tw_split;
   const int shn = LOGN == TILE_LOGS ? 0 : c.log_split - LOGN;
-  auto load = [&](int, int q, int s) {
-    const int i = q + (s << PL::first_shift);
-    float2 z;
-    if constexpr (P == 2) {                                 // y[2k] from buf[i] + buf[i + S], y[2k+1] from the difference
-      const float2 a = cmul(__ldg(&m.w[i + S]), __ldg(&m.X[i + S]));
-      const float2 b = cmul(__ldg(&m.w[i]), __ldg(&m.X[i]));
-      if (r == 0) return cadd(a, b);
-      z = csub(a, b);
-    } else {
+  float2 z;
+  if constexpr (P == 2) {                                   // y[2k] from buf[i] + buf[i + S], y[2k+1] from the difference
+    const float2 a = cmul(__ldg(&m.w[i + S]), __ldg(&m.X[i + S]));
+    const float2 b = cmul(__ldg(&m.w[i]), __ldg(&m.X[i]));
+    if (r == 0) return cadd(a, b);
+    z = csub(a, b);
+  } else {
 #pragma unroll
-      for (int mm = 0; mm < P; ++mm) {
-        const int j = i + (((mm + P / 2) & (P - 1)) << LOGS);
-        const float2 b = cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
-        z = mm ? cadd(z, rot_inv<P>(b, (mm * r) & (P - 1))) : b;
-      }
-      if (r == 0) return z;
+    for (int mm = 0; mm < P; ++mm) {
+      const int j = i + (((mm + P / 2) & (P - 1)) << LOGS);
+      const float2 b = cmul(__ldg(&m.w[j]), __ldg(&m.X[j]));
+      z = mm ? cadd(z, rot_inv<P>(b, (mm * r) & (P - 1))) : b;
     }
-    const float2 t = __ldg(&twn[(i * r) << shn]);
-    return cmul(z, make_float2(t.x, -t.y));
-  };
+    if (r == 0) return z;
+  }
+  const float2 t = __ldg(&twn[(i * r) << shn]);
+  return cmul(z, make_float2(t.x, -t.y));
+}
+
+template <int S, int T, int LOGP>
+__device__ __forceinline__ void fcfb_tile_part(float2* sm, const TileMeta* meta, const FcfbTileConst& c) {
+  constexpr int LOGS = ilog2c(S), P = 1 << LOGP;
+  using PL = StagePlan<LOGS, S / T>;
+  constexpr int RL = 1 << PL::last;
+  const TileMeta& m = meta[0];
+  auto load = [&](int, int q, int s) { return part_input<S, LOGP>(m, c, q + (s << PL::first_shift)); };
   auto store = [&](int, int q, int u, float2 v) {
-    fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[P * k + r] = v; });
+    fcfb_keep<LOGS, RL>(q, u, [&](int k) { m.out[P * k + m.pad] = v; });
   };
   tile_pipeline<LOGS, S, T, +1, true>(sm, 1, c.tw, load, store);
 }
@@ -455,50 +458,6 @@ __device__ __forceinline__ void fcfb_tile_chirp(float2* sm, const TileMeta* meta
     if ((unsigned)k < (unsigned)keep) meta[t].out[k] = cmul(v, __ldg(&chirp[o]));
   };
   tile_chirp<LOGM, S, T>(sm, count, c.tw, load, H, store);
-}
-
-template <int S, int T, bool CHIRP>
-__device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const TileMeta* meta, int count,
-                                                   const FcfbTileConst& c, const BluDesc* bd) {
-  constexpr int LOGS = ilog2c(S);
-  if constexpr (CHIRP) {
-    switch (log2n - BLU_TAG) {
-      case 4: fcfb_tile_chirp<4, S, T>(sm, meta, count, c, bd); break;
-      case 5: fcfb_tile_chirp<5, S, T>(sm, meta, count, c, bd); break;
-      case 6: fcfb_tile_chirp<6, S, T>(sm, meta, count, c, bd); break;
-      case 7: fcfb_tile_chirp<7, S, T>(sm, meta, count, c, bd); break;
-      case 8: fcfb_tile_chirp<8, S, T>(sm, meta, count, c, bd); break;
-      case 9: fcfb_tile_chirp<9, S, T>(sm, meta, count, c, bd); break;
-      case 10: fcfb_tile_chirp<10, S, T>(sm, meta, count, c, bd); break;
-      case 11: fcfb_tile_chirp<11, S, T>(sm, meta, count, c, bd); break;
-      case 12: if constexpr (LOGS >= 12) fcfb_tile_chirp<12, S, T>(sm, meta, count, c, bd); break;
-      case 13: if constexpr (LOGS >= 13) fcfb_tile_chirp<13, S, T>(sm, meta, count, c, bd); break;
-    }
-    return;
-  } else {
-  if (log2n > LOGS) {
-    switch (log2n - LOGS) {
-      case 1: fcfb_tile_part<S, T, 1>(sm, meta, c); break;
-      case 2: fcfb_tile_part<S, T, 2>(sm, meta, c); break;
-      case 3: fcfb_tile_part<S, T, 3>(sm, meta, c); break;
-    }
-    return;
-  }
-  switch (log2n) {
-    case 2: fcfb_tile<2, S, T>(sm, meta, count, c); break;
-    case 3: fcfb_tile<3, S, T>(sm, meta, count, c); break;
-    case 4: fcfb_tile<4, S, T>(sm, meta, count, c); break;
-    case 5: fcfb_tile<5, S, T>(sm, meta, count, c); break;
-    case 6: fcfb_tile<6, S, T>(sm, meta, count, c); break;
-    case 7: fcfb_tile<7, S, T>(sm, meta, count, c); break;
-    case 8: fcfb_tile<8, S, T>(sm, meta, count, c); break;
-    case 9: fcfb_tile<9, S, T>(sm, meta, count, c); break;
-    case 10: fcfb_tile<10, S, T>(sm, meta, count, c); break;
-    case 11: fcfb_tile<11, S, T>(sm, meta, count, c); break;
-    case 12: if constexpr (LOGS >= 12) fcfb_tile<12, S, T>(sm, meta, count, c); break;
-    case 13: if constexpr (LOGS >= 13) fcfb_tile<13, S, T>(sm, meta, count, c); break;
-  }
-  }
 }
 
 }  // namespace sk

@@ -23,6 +23,7 @@
 #include "sk_types.h"
 #include "sk_fft.cuh"
 #include "sk_fcfb.cuh"
+#include "sk_fcfb_ip.cuh"
 
 namespace sk {
 
