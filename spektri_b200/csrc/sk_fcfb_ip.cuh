@@ -134,10 +134,12 @@ __device__ __forceinline__ void fcfb_tile_ip(float2* sm, const TileMeta* meta, i
 //   last : X[k''' + 4096 u1]       = DFT_2 over i1 of W_8192^(i1 k''') Z2[i1][k''']         (k''' = k'' + 256 u2)
 // Y[q][k4] at q + 513 k4; A and B write in place, so Z2[i1][k4 + 16 u3 + 256 u2]
 // sits at i1 + 2 u2 + 32 u3 + 513 k4.  Lanes run k4 fastest in A, B and the
-// last stage (odd stride 513), consecutive q in the leaf.
+// last stage (odd stride 513), consecutive q in the leaf.  DIR = +1 is the
+// inverse transform (the filter bank), -1 the forward one (the row pass of
+// the two-pass forward FFT).
 constexpr int IP8K_ROW = 513, IP8K_SPAN = 8192 + 16;
 
-template <int T, class Load, class Store>
+template <int T, int DIR = +1, class Load, class Store>
 __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restrict__ tw, Load& load, Store& store) {
   static_assert(T == 512, "one 16-point leaf, A and B butterfly per thread");
   const int tid = threadIdx.x;
@@ -145,7 +147,7 @@ __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restr
     float2 v[16];
 #pragma unroll
     for (int s = 0; s < 16; ++s) v[s] = load(0, tid, s);
-    dft<16, +1>(v);
+    dft<16, DIR>(v);
     float2* p = sm + tid;
 #pragma unroll
     for (int k = 0; k < 16; ++k) p[k * IP8K_ROW] = v[k];
@@ -157,7 +159,7 @@ __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restr
     float2 v[16];
 #pragma unroll
     for (int s = 0; s < 16; ++s) v[s] = p[32 * s];
-    twiddle_dft<16, TILE_LOGS - 8, +1>(v, tw, k4);          // P = 256, span 16
+    twiddle_dft<16, TILE_LOGS - 8, DIR>(v, tw, k4);          // P = 256, span 16
 #pragma unroll
     for (int u = 0; u < 16; ++u) p[32 * u] = v[u];
   }
@@ -168,7 +170,7 @@ __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restr
     float2 v[16];
 #pragma unroll
     for (int s = 0; s < 16; ++s) v[s] = p[2 * s];
-    twiddle_dft<16, TILE_LOGS - 12, +1>(v, tw, tid & 255);  // P = 4096, span 256: k'' = k4 + 16 u3
+    twiddle_dft<16, TILE_LOGS - 12, DIR>(v, tw, tid & 255);  // P = 4096, span 256: k'' = k4 + 16 u3
 #pragma unroll
     for (int u = 0; u < 16; ++u) p[2 * u] = v[u];
   }
@@ -178,7 +180,7 @@ __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restr
     const int kk = tid + bb * T;                             // k''' < 4096
     const float2* p = sm + 2 * (kk >> 8) + 32 * ((kk >> 4) & 15) + IP8K_ROW * (kk & 15);
     float2 v[2] = {p[0], p[1]};
-    twiddle_dft<2, 0, +1>(v, tw, kk);                        // P = 8192, span 4096
+    twiddle_dft<2, 0, DIR>(v, tw, kk);                        // P = 8192, span 4096
     store(0, kk, 0, v[0]);
     store(0, kk, 1, v[1]);
   }

@@ -44,7 +44,7 @@ cudaError_t fwd_col_launch_one(int grid, const FwdArgs& a, float2* Y, cudaStream
     const long long cols = (long long)a.B << TILE_LOGS;
     fwd_colreg_kernel<FMT><<<(unsigned)((cols + 255) / 256), 256, 0, st>>>(a, Y);
   } else {
-    fwd_col_kernel<TILE_S, TILE_T, FMT><<<grid, TILE_T, TILE_SMEM_COL, st>>>(a, Y);
+    fwd_col_kernel<TILE_S, TILE_T16, FMT><<<grid, TILE_T16, TILE_SMEM_COL, st>>>(a, Y);
   }
   return cudaGetLastError();
 }
@@ -54,7 +54,7 @@ cudaError_t fwd_prepare_one() {
   cudaError_t e = cudaFuncSetAttribute(fwd_fft_kernel<TILE_S, TILE_T, FMT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(fwd_col_kernel<TILE_S, TILE_T, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(fwd_col_kernel<TILE_S, TILE_T16, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)TILE_SMEM_COL);
 }
 
@@ -64,7 +64,7 @@ template <int FMT>
 const void* fwd_ptr_one(int kind, int R1) {
   if (kind == 3) return fwd_colmix_ptr<FMT>(R1);
   if (kind == 2) return (const void*)fwd_colreg_kernel<FMT>;
-  return kind ? (const void*)fwd_col_kernel<TILE_S, TILE_T, FMT> : (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
+  return kind ? (const void*)fwd_col_kernel<TILE_S, TILE_T16, FMT> : (const void*)fwd_fft_kernel<TILE_S, TILE_T, FMT>;
 }
 
 }  // namespace sk

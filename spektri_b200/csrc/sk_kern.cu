@@ -61,9 +61,9 @@ cudaError_t launch_fwd_rows(int grid, const FwdArgs& a, const float2* Y, cudaStr
   FwdArgs args = a;
   const float2* y = Y;
   void* params[] = {(void*)&args, (void*)&y};
-  const void* fn = a.log2R1 < 0 ? (const void*)fwd_rowmix_kernel<TILE_S, TILE_T> : (const void*)fwd_row_kernel<TILE_S, TILE_T>;
-  return launch_kernel(fn, dim3(grid), dim3(TILE_T), params, TILE_SMEM, st,
-                       pdl);
+  const bool mix = a.log2R1 < 0;
+  const void* fn = mix ? (const void*)fwd_rowmix_kernel<TILE_S, TILE_T> : (const void*)fwd_row_kernel<TILE_T16>;
+  return launch_kernel(fn, dim3(grid), dim3(mix ? TILE_T : TILE_T16), params, TILE_SMEM, st, pdl);
 }
 
 // Up to WELCH_BINS_MAX_B blocks per buffer each warp walks its own bins over
@@ -134,7 +134,7 @@ cudaError_t fcfb_prepare() {
       if (e != cudaSuccess) return e;
     }
   const void* fns[] = {(const void*)fcfb_bwd_fft_kernel<TILE_S, TILE_T>,
-                       (const void*)fwd_row_kernel<TILE_S, TILE_T>, (const void*)fwd_rowmix_kernel<TILE_S, TILE_T>};
+                       (const void*)fwd_row_kernel<TILE_T16>, (const void*)fwd_rowmix_kernel<TILE_S, TILE_T>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_SMEM);
     if (e != cudaSuccess) return e;

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
 // Pass B (rows): S-point FFT of row k1 of Y gives Z[k1 + R1 k2], stored at
 // k1 S + k2 — the residue layout the spectrum split reads.
 template <int S, int T, int FMT>
-__global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {
+__global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {   // T = 512: 16 elements per thread
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
   constexpr int E = S / T, LOGS = ilog2c(S);
@@ -395,12 +395,18 @@ __device__ __forceinline__ void fwd_rows_tile(float2* sm, const FwdArgs& a, cons
   tile_pipeline<LOGM, S, T, -1, false>(sm, count, a.tw_tile, load, store);
 }
 
-// Rows of S points (the power-of-two two-pass FFT) ...
-template <int S, int T>
+// Rows of 8192 points (the power-of-two two-pass FFT): one row per tile, on
+// the in-place 16-16-16-2 pipeline with 512 threads (16 elements each, two
+// CTAs per SM at 64 registers).
+template <int T>
 __global__ void __launch_bounds__(T, 2) fwd_row_kernel(FwdArgs a, const float2* Y) {
   extern __shared__ float2 sm[];
   pdl_wait();                                               // Y from the column pass
-  fwd_rows_tile<ilog2c(S), S, T>(sm, a, Y, blockIdx.x);
+  const float2* Yr = Y + ((size_t)blockIdx.x << TILE_LOGS);
+  float2* Zr = a.Z + ((size_t)blockIdx.x << TILE_LOGS);
+  auto load = [&](int, int q, int s) { return __ldg(&Yr[q + (s << 9)]); };
+  auto store = [&](int, int kk, int u, float2 v) { Zr[kk + (u << 12)] = v; };
+  ip_pipeline_8k<T, -1>(sm, a.tw_tile, load, store);
   trace_end(a.trace, 1);
 }
 

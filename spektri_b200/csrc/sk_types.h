@@ -10,6 +10,7 @@ namespace sk {
 
 constexpr int TILE_S = 8192;              // complex elements per FFT tile
 constexpr int TILE_T = 256;               // threads per tile CTA (32 elements each)
+constexpr int TILE_T16 = 512;             // threads of the 16-element kernels (two-pass column and row passes)
 constexpr int TILE_LOGS = 13;
 constexpr int MAX_TILE_TRANSFORMS = 128;  // transforms per filter-bank tile
 constexpr int MAX_SPLIT_LOG = 3;          // an IFFT of up to 2^3 tiles runs as independent parts (n = P S, P <= 8)
