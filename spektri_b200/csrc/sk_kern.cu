@@ -74,7 +74,11 @@ const void* welch_ptr_t(bool cplx, int B) {
     return cplx ? (const void*)welch_bins_kernel<false, P2> : (const void*)welch_bins_kernel<true, P2>;
   return cplx ? (const void*)welch_kernel<false, P2> : (const void*)welch_kernel<true, P2>;
 }
-const void* welch_kernel_ptr(bool cplx, int B, bool pow2) {
+// Complex spectra of the power-of-two two-pass FFT with R1 >= 16 rows per
+// block: the transposing kernel (its reads of the residue layout coalesce).
+bool welch_transposed(bool cplx, bool pow2, int R1) { return cplx && pow2 && R1 >= 16; }
+const void* welch_kernel_ptr(bool cplx, int B, bool pow2, int R1) {
+  if (welch_transposed(cplx, pow2, R1)) return (const void*)welch_tr_kernel<256>;
   return pow2 ? welch_ptr_t<true>(cplx, B) : welch_ptr_t<false>(cplx, B);
 }
 
@@ -100,12 +104,16 @@ cudaError_t launch_extend(bool cplx, int B, const float2* X, int K, int N, float
 }
 
 cudaError_t launch_welch(bool cplx, const WelchArgs& w, cudaStream_t st, bool pdl) {
-  const int bins_per_cta = w.B <= WELCH_BINS_MAX_B ? WELCH_WARP_BINS * WELCH_WARPS : WELCH_WARP_BINS;
-  const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
+  const bool pow2 = (w.s.N & (w.s.N - 1)) == 0;
   WelchArgs args = w;
   void* params[] = {(void*)&args};
-  return launch_kernel(welch_kernel_ptr(cplx, w.B, (w.s.N & (w.s.N - 1)) == 0), dim3(g), dim3(32 * WELCH_WARPS),
-                       params, 0, st, pdl);
+  if (welch_transposed(cplx, pow2, w.s.R1))
+    return launch_kernel(welch_kernel_ptr(cplx, w.B, pow2, w.s.R1), dim3(w.s.K / WT_BINS), dim3(256), params, 0, st,
+                         pdl);
+  const int bins_per_cta = w.B <= WELCH_BINS_MAX_B ? WELCH_WARP_BINS * WELCH_WARPS : WELCH_WARP_BINS;
+  const int g = (w.s.K + bins_per_cta - 1) / bins_per_cta;
+  return launch_kernel(welch_kernel_ptr(cplx, w.B, pow2, w.s.R1), dim3(g), dim3(32 * WELCH_WARPS), params, 0, st,
+                       pdl);
 }
 
 // Filter-bank tile shapes (tile size x threads, minimum CTAs per SM):

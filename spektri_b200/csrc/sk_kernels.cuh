@@ -632,6 +632,67 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
   trace_end(a.trace, 2);
 }
 
+// The same records for complex input whose spectra come from the two-pass
+// FFT (R1 = Nc / M >= 16, powers of two): element m = k1 + R1 k2 sits at
+// k1 M + k2, so the bins of a warp in welch_bins_kernel would read 32
+// different rows.  Here a CTA owns WT_BINS consecutive bins m0 .. m0 +
+// WT_BINS - 1, i.e. k2 in [k20, k20 + W) of every row k1 (W = WT_BINS / R1):
+// per block it reads the R1 row segments of W elements (lanes along a
+// segment: coalesced), transposes them through shared memory into bin order
+// (one pad slot per R1 bins against bank conflicts), and each thread then
+// forms, accumulates and emits its bins (tid + i T) exactly as
+// welch_bins_kernel does, with coalesced spectrum, accumulator and record
+// accesses.  Blocks run in order, one barrier pair per block.
+constexpr int WT_BINS = 1024;
+template <int T>
+__global__ void __launch_bounds__(T) welch_tr_kernel(WelchArgs a) {
+  constexpr int PER = WT_BINS / T;
+  __shared__ float2 zs[WT_BINS + WT_BINS / 16 + 2];         // bins m0 - 1 .. m0 + WT_BINS, padded
+  pdl_wait();                                               // Z from the forward FFT
+  const SplitArgs& s = a.s;
+  const int logR1 = s.log2R1, logW = ilog2c(WT_BINS) - logR1, W = 1 << logW;
+  const int m0 = blockIdx.x * WT_BINS, k20 = m0 >> logR1;
+  // bin offset o (o = -1 .. WT_BINS) -> slot; one pad slot after every R1 bins
+  auto slot = [&](int o) { return 1 + o + ((o + 1) >> logR1); };
+  float acc[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) acc[i] = a.acc[m0 + threadIdx.x + i * T];
+  int cnt = a.accn0, r = 0;
+  for (int b = 0; b < a.B; ++b) {
+    const float2* Zb = s.Z + (size_t)b * s.Nc;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = threadIdx.x + i * T, k1 = e >> logW, j = e & (W - 1);
+      zs[slot(k1 + (j << logR1))] = __ldg(&Zb[((size_t)k1 << s.logM) + k20 + j]);
+    }
+    if (threadIdx.x == 0) zs[slot(-1)] = z_at<true>(s, Zb, (m0 - 1) & (s.N - 1));
+    if (threadIdx.x == 1) zs[slot(WT_BINS)] = z_at<true>(s, Zb, (m0 + WT_BINS) & (s.N - 1));
+    __syncthreads();
+    float2* Xb = s.X + (size_t)b * a.xs;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = threadIdx.x + i * T;
+      const float2 x0 = zs[slot(e - 1)], x1 = zs[slot(e)], x2 = zs[slot(e + 1)];
+      store_ext<false>(Xb, s.N, a.maxn, m0 + e, x1);
+      const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
+      acc[i] += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
+    }
+    if (++cnt >= a.averages) {
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        emit_record(a, r, m0 + threadIdx.x + i * T, acc[i], cnt);
+        acc[i] = 0.0f;
+      }
+      cnt = 0;
+      ++r;
+    }
+    __syncthreads();                                        // zs is rewritten for the next block
+  }
+#pragma unroll
+  for (int i = 0; i < PER; ++i) a.acc[m0 + threadIdx.x + i * T] = acc[i];
+  trace_end(a.trace, 2);
+}
+
 // ----------------------------------------------------------------- filter bank
 // CHIRP: the chirp-z tiles of the list (their own launch); else the
 // power-of-two tiles.

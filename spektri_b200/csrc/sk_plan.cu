@@ -489,7 +489,7 @@ int run_graph(sk_plan* pl, const uint8_t* raw, const WelchCall& wc, cudaStream_t
     std::vector<cudaGraphNode_t> nodes(n);
     cudaGraphGetNodes(g, nodes.data(), &n);
     const void* f_fwd = fwd_kernel_ptr(pl->fmt, fwd_kind(pl), pl->R1);
-    const void* f_welch = welch_kernel_ptr(pl->cplx, pl->B, pl->log2N >= 0);
+    const void* f_welch = welch_kernel_ptr(pl->cplx, pl->B, pl->log2N >= 0, pl->R1);
     for (auto nd : nodes) {
       cudaGraphNodeType t;
       if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;

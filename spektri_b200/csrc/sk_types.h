@@ -198,6 +198,6 @@ const void* fwd_kernel_ptr_16(int fmt, int kind, int R1);
 const void* fwd_kernel_ptr_32(int fmt, int kind, int R1);
 // Mixed-radix column factors: R1 = R0 * P with R0 = 3 or 5 and P a power of two.
 constexpr bool mixed_r1_ok(int r1) { return r1 == 3 || r1 == 5 || r1 == 6 || r1 == 10 || r1 == 12; }
-const void* welch_kernel_ptr(bool cplx, int B, bool pow2);   // pow2: the FFT size is a power of two
+const void* welch_kernel_ptr(bool cplx, int B, bool pow2, int R1);   // pow2: the FFT size is a power of two
 
 }  // namespace sk
