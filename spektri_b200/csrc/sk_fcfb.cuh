@@ -41,8 +41,10 @@ __host__ __device__ constexpr int stage_log_radix(int logn, int e, int p) {
     return p < 3 ? t[logn - 2][p] : 0;
   }
   // radix <= 16: ... 512:[8,8,8] 1024:[16,8,8] 2048:[16,16,8] 4096:[16,16,16] 8192:[16,16,16,2]
-  constexpr int u[12][4] = {{2, 0, 0, 0}, {3, 0, 0, 0}, {4, 0, 0, 0}, {3, 2, 0, 0}, {3, 3, 0, 0}, {4, 3, 0, 0},
-                            {4, 4, 0, 0}, {3, 3, 3, 0}, {4, 3, 3, 0}, {4, 4, 3, 0}, {4, 4, 4, 0}, {4, 4, 4, 1}};
+  // 16384:[16,16,16,4] (the chirp-z tiles of M = 16384)
+  constexpr int u[13][4] = {{2, 0, 0, 0}, {3, 0, 0, 0}, {4, 0, 0, 0}, {3, 2, 0, 0}, {3, 3, 0, 0}, {4, 3, 0, 0},
+                            {4, 4, 0, 0}, {3, 3, 3, 0}, {4, 3, 3, 0}, {4, 4, 3, 0}, {4, 4, 4, 0}, {4, 4, 4, 1},
+                            {4, 4, 4, 2}};
   return u[logn - 2][p];
 }
 
@@ -153,7 +155,9 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
                                            const Pad& pad = Pad()) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   constexpr int SH = TILE_LOGS - LOGL - LOGR;            // stage tables: P = 2^(LOGL + LOGR)
-  static_assert(NB >= 1 && SH >= 0, "bad stage");
+  // SH = -1: the span-4096 radix-4 stage of a 16384-point transform, whose
+  // twiddle powers come from the appended p = 14 table (w^1 only)
+  static_assert(NB >= 1 && (SH >= 0 || (SH == -1 && R <= 4)), "bad stage");
   auto twiddled_dft = [&](float2* v, int j) {            // DFT_R(v[s] w^s); no twiddle for LOGL = 0
     if constexpr (LOGL > 0) twiddle_dft<R, SH, DIR>(v, tw, j);
     else dft<R, DIR>(v);

@@ -221,13 +221,16 @@ __device__ __forceinline__ void fcfb_tile_part_ip(float2* sm, const TileMeta* me
 // per thread, n = 512 .. 4096 run on the in-place pipeline, n = 8192 natively
 // in an 8192-point tile (as two parts in a 4096-point one) and n > S as parts
 // of S points on the in-place pipeline; smaller n, the 32-element shape and
-// the chirp-z tiles run on the Stockham stages.
+// the chirp-z tiles run on the Stockham stages (M = 16384 chirp-z tiles in a
+// kernel of their own: one 16384-point tile per CTA, 1024 threads).
 template <int S, int T, bool CHIRP>
 __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const TileMeta* meta, int count,
                                                    const FcfbTileConst& c, const BluDesc* bd) {
   constexpr int LOGS = ilog2c(S);
   constexpr bool IP = S / T == 16;
-  if constexpr (CHIRP) {
+  if constexpr (CHIRP && LOGS == CHIRP_LOGM_MAX) {
+    fcfb_tile_chirp<CHIRP_LOGM_MAX, S, T>(sm, meta, count, c, bd);   // the 16384-point tiles' own kernel
+  } else if constexpr (CHIRP) {
     switch (log2n - BLU_TAG) {
       case 4: fcfb_tile_chirp<4, S, T>(sm, meta, count, c, bd); break;
       case 5: fcfb_tile_chirp<5, S, T>(sm, meta, count, c, bd); break;

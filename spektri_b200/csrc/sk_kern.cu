@@ -141,6 +141,11 @@ cudaError_t fcfb_prepare() {
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcfb_smem(sh[0]));
       if (e != cudaSuccess) return e;
     }
+  {
+    const cudaError_t e = cudaFuncSetAttribute(fcfb_ptr_16384_chirp(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)fcfb_smem(1 << CHIRP_LOGM_MAX));
+    if (e != cudaSuccess) return e;
+  }
   const void* fns[] = {(const void*)fcfb_bwd_fft_kernel<TILE_S, TILE_T>,
                        (const void*)fwd_row_kernel<TILE_T16>, (const void*)fwd_rowmix_kernel<TILE_S, TILE_T>};
   for (const void* f : fns) {
@@ -148,6 +153,14 @@ cudaError_t fcfb_prepare() {
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_fcfb_chirp16k(int grid, const FcfbArgs& a, int tile_base, cudaStream_t st) {
+  FcfbArgs args = a;
+  int base = tile_base;
+  void* params[] = {(void*)&args, (void*)&base};
+  return launch_kernel(fcfb_ptr_16384_chirp(), dim3(grid), dim3(1024), params, fcfb_smem(1 << CHIRP_LOGM_MAX), st,
+                       false);
 }
 
 cudaError_t fcfb_occupancy(int tile_size, int tile_threads, int* per_sm) {

@@ -129,6 +129,7 @@ struct sk_plan {
     std::vector<int> plain_start, plain_count;
   };
   TileSet ts[2];                        // 8192-point tiles (also the adjoint's) and 4096-point tiles
+  TileSet t16;                          // chirp-z tiles of M = 16384 (one transform each, their own kernel)
   int* d_cursor = nullptr;              // persistent tile cursors: power-of-two, chirp-z
   int persist_grid = 1;
   int sms = 1;                          // multiprocessors of the device
@@ -167,7 +168,7 @@ int plan_free(sk_plan* pl) {
   DeviceGuard g(pl->p.device);
   void* ptrs[] = {pl->d_tw_tile, pl->d_tw_big, pl->d_tw_split, pl->d_halo[0], pl->d_halo[1], pl->d_Z, pl->d_Y, pl->d_X,
                   pl->d_acc, pl->d_w, pl->d_chans, pl->d_chans_aux, pl->d_bwd, pl->ts[0].d_tiles, pl->ts[0].d_list,
-                  pl->ts[1].d_tiles, pl->ts[1].d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec,
+                  pl->ts[1].d_tiles, pl->ts[1].d_list, pl->t16.d_tiles, pl->t16.d_list, pl->d_cursor, pl->d_raw, pl->d_out, pl->d_spec,
                   pl->d_blu, pl->d_blu_tab, pl->d_trace, pl->d_bwd_g, pl->d_bin_off, pl->d_bin_ent};
   if (pl->h_trace) cudaFreeHost(pl->h_trace);
   if (pl->graph_exec) cudaGraphExecDestroy(pl->graph_exec);
@@ -200,10 +201,15 @@ void twiddles(std::vector<float2>& t, long long n) {
 }
 
 // The tile twiddle array: W_S^k, then the per-stage tables W_P^(j s)
-// (layout: stage_tw_offset).
+// (layout: stage_tw_offset), then W_16384^j (j < 8192) for the last stage of
+// the 16384-point chirp-z tiles.
 void tile_twiddles(std::vector<float2>& t) {
   twiddles(t, TILE_S);
-  t.resize(TILE_TW_ELEMS);
+  t.resize(TILE_TW_ELEMS_X);
+  for (int j = 0; j < (1 << TILE_LOGS); ++j) {       // p = 14, si = 0: W_16384^j
+    const double a = -2.0 * M_PI * (double)j / (double)(1 << CHIRP_LOGM_MAX);
+    t[(size_t)(TILE_TW_ELEMS + j)] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
   static const int pw[3] = {1, 4, 16};
   for (int p = 1; p <= TILE_LOGS; ++p) {
     const long long P = 1ll << p, h = P / 2;
@@ -341,12 +347,12 @@ int launch_forward(sk_plan* pl, const uint8_t* raw, float2* X, const WelchCall* 
 
 // Chirp-z transform size for IFFT size n: the smallest M = 2^logm with
 // M >= n + keep - 1, keep = 6(n/8) (the circular convolution then matches
-// the linear one on every kept output [n/8, 7(n/8))).  0 when M > 8192.
+// the linear one on every kept output [n/8, 7(n/8))).  0 when M > 16384.
 int chirp_logm(long long n) {
   const long long need = n + 6 * (n / 8) - 1;
   int lm = 4;
   while ((1ll << lm) < need) ++lm;
-  return lm <= TILE_LOGS ? lm : 0;
+  return lm <= CHIRP_LOGM_MAX ? lm : 0;
 }
 
 // In-place radix-2 FFT in double (host; chirp-z kernel spectra only).
@@ -447,16 +453,34 @@ cudaError_t launch_batched(sk_plan* pl, const FcfbArgs& a0, int size, int thread
   return e;
 }
 
+// The chirp-z tiles of M = 16384 (their own kernel, after the others in
+// stream order): all of them (batched), or channel c's (c >= 0).
+int launch_t16(sk_plan* pl, const FcfbArgs& a0, int c, cudaStream_t st) {
+  const sk_plan::TileSet& t = pl->t16;
+  const int base = c < 0 ? 0 : t.plain_start[c], n = c < 0 ? t.n_batched : t.plain_count[c];
+  if (n == 0) return SK_OK;
+  FcfbArgs a = a0;
+  a.tiles = t.d_tiles;
+  a.list = t.d_list;
+  SK_CUDA(launch_fcfb_chirp16k(n, a, base, st));
+  return SK_OK;
+}
+
 int run_fcfb(sk_plan* pl, const ChanDev* chans, const float2* X, bool batched, cudaStream_t st, bool graph = false) {
   if (pl->ch.empty()) return SK_OK;
   FcfbArgs a = fcfb_args(pl, chans, X);
   const sk_plan::TileSet& t = cur_tiles(pl);
   if (batched) {
-    SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st, graph));
+    const sk_plan::TileSet& tb = pl->ts[pl->fcfb_size == TILE_S ? 0 : 1];
+    if (tb.n_batched > 0) SK_CUDA(launch_batched(pl, a, pl->fcfb_size, pl->fcfb_threads, pl->persist_grid, st, graph));
+    TRY_NOFREE(launch_t16(pl, a, -1, st));
   } else {
-    for (size_t c = 0; c < pl->ch.size(); ++c)
-      SK_CUDA(launch_fcfb(false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
-                          t.plain_start[c], st));
+    for (size_t c = 0; c < pl->ch.size(); ++c) {
+      if (t.plain_count[c] > 0)
+        SK_CUDA(launch_fcfb(false, pl->ch[c].log2n == 0, pl->fcfb_size, pl->fcfb_threads, t.plain_count[c], a,
+                            t.plain_start[c], st));
+      TRY_NOFREE(launch_t16(pl, a, (int)c, st));
+    }
   }
   return SK_OK;
 }
@@ -620,7 +644,7 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       if (!pow2 && (bins < 4 || bins % 4 != 0 || lm == 0)) {
         st = SK_ERR_UNSUPPORTED;
         fprintf(stderr, "Error creating filter: IFFT size %lld not supported on the device (powers of two up to %d, "
-                "other multiples of 4 up to 4680)\n", bins, 1 << MAX_IFFT_LOG);
+                "other multiples of 4 up to 9364)\n", bins, 1 << MAX_IFFT_LOG);
       } else {
         sk_plan::Chan c;
         c.n = (uint32_t)bins;
@@ -823,6 +847,11 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
     for (size_t c = 0; c < pl->ch.size(); ++c) {
       const sk_plan::Chan& ch = pl->ch[c];
       const bool chirp = ch.log2n == 0;
+      if (chirp && ch.logm > TILE_LOGS) {             // M = 16384: in t16 below
+        t.plain_start.push_back((int)tiles.size());
+        t.plain_count.push_back(0);
+        continue;
+      }
       const int l2 = chirp ? 0 : ch.log2n;
       const int per = chirp ? std::max(1, std::min(t.size >> std::min(ch.logm, logt), MAX_TILE_TRANSFORMS)) : per_tile(l2);
       const int base = (int)list.size();
@@ -840,6 +869,29 @@ int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_
       CUDA_TRY(cudaMemcpy(t.d_list, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice));
     if (!tiles.empty())
       CUDA_TRY(cudaMemcpy(t.d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
+  }
+  {  // chirp-z channels of M = 16384: one transform per tile, in channel then block order
+    sk_plan::TileSet& t = pl->t16;
+    t.size = 1 << CHIRP_LOGM_MAX;
+    std::vector<int2> list;
+    std::vector<TileDesc> tiles;
+    for (size_t c = 0; c < pl->ch.size(); ++c) {
+      const sk_plan::Chan& ch = pl->ch[c];
+      t.plain_start.push_back((int)tiles.size());
+      if (ch.log2n == 0 && ch.logm == CHIRP_LOGM_MAX)
+        for (int b = 0; b < pl->B; ++b) {
+          tiles.push_back(TileDesc{BLU_TAG + ch.logm, (int)list.size(), 1, ch.blu});
+          list.push_back(make_int2((int)c, b));
+        }
+      t.plain_count.push_back((int)tiles.size() - t.plain_start.back());
+    }
+    t.n_batched = t.n_chirp = (int)tiles.size();
+    if (!tiles.empty()) {
+      TRY(dev_alloc(&t.d_list, list.size()));
+      TRY(dev_alloc(&t.d_tiles, tiles.size()));
+      CUDA_TRY(cudaMemcpy(t.d_list, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(t.d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
+    }
   }
   int sms = 0, per_sm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
@@ -890,8 +942,11 @@ int sk_plan_channel(const sk_plan* pl, int32_t c, sk_channel_info* info) {
 
 int sk_launches_per_call(const sk_plan* pl) {
   if (!pl) return fail(SK_ERR_ARG, "null plan");
+  const sk_plan::TileSet& t = cur_tiles(pl);
   const int fb = pl->ch.empty() ? 0
-                 : (pl->p.mode == SK_MODE_BATCHED ? 1 + (pl->h_blu.empty() ? 0 : 1) : (int)pl->ch.size());
+                 : pl->p.mode == SK_MODE_BATCHED
+                     ? (t.n_chirp > 0) + (t.n_batched > t.n_chirp) + (pl->t16.n_batched > 0)
+                     : (int)pl->ch.size();
   return (pl->R1 > 1 ? 3 : 2) + fb;
 }
 
@@ -1097,6 +1152,7 @@ int sk_fcfb_forward_device(sk_plan* pl, const float* X, const float* const* W, f
   if (t.n_batched > t.n_chirp)
     SK_CUDA(launch_fcfb(false, false, pl->fcfb_size, pl->fcfb_threads, t.n_batched - t.n_chirp, a,
                         t.n_chirp, st));
+  TRY_NOFREE(launch_t16(pl, a, -1, st));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }

@@ -23,6 +23,11 @@ __host__ __device__ constexpr int stage_tw_offset(int p, int si) {
   return TILE_S + 3 * ((1 << (p - 1)) - 1) + si * (1 << (p - 1));
 }
 constexpr int TILE_TW_ELEMS = TILE_S + 3 * ((1 << TILE_LOGS) - 1);   // p = 1 .. 13
+// The filter bank's array appends the p = 14 table for si = 0 (W_16384^j,
+// j < 8192, at stage_tw_offset(14, 0) = TILE_TW_ELEMS): the last radix-4
+// stage of the 16384-point chirp-z tiles reads only it.
+constexpr int TILE_TW_ELEMS_X = TILE_TW_ELEMS + (1 << TILE_LOGS);
+constexpr int CHIRP_LOGM_MAX = TILE_LOGS + 1;   // chirp-z transforms up to M = 16384 (IFFT sizes up to 9364)
 // Tile in shared memory: S complex values with one pad slot per 16.
 constexpr size_t TILE_SMEM = sizeof(float2) * (size_t)(TILE_S + TILE_S / 16);
 // The column pass's tile adds one slot per transform (at most S/16 of them).
@@ -185,6 +190,9 @@ const void* fcfb_ptr_8192x512(bool persistent);
 const void* fcfb_ptr_8192x512_chirp(bool persistent);
 const void* fcfb_ptr_4096(bool persistent);
 const void* fcfb_ptr_4096_chirp(bool persistent);
+const void* fcfb_ptr_16384_chirp();                       // non-persistent, M = 16384 chirp-z tiles only
+// One launch of that kernel: grid = tiles (one transform each) from tile_base.
+cudaError_t launch_fcfb_chirp16k(int grid, const FcfbArgs& a, int tile_base, cudaStream_t st);
 // Adjoint in three deterministic launches: the per-transform forward FFTs of
 // the padded output gradients (grid = tiles), dW summed over blocks in block
 // order (grid = channels x n_max/256), dX gathered per bin in channel order.

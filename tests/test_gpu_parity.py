@@ -135,7 +135,7 @@ def test_edge_channels_wrap_mirror_and_drops():
         dict(fs_out=64e3, fc_out=1001e3),               # centre not a multiple of 4: dropped
         dict(fs_out=48e3, fc_out=0.0),                  # n = 48: not a power of two (chirp-z)
         dict(fs_out=-4e3, fc_out=0.0),                  # bins <= 0: dropped
-        dict(fs_out=4684e3, fc_out=0.0),                # n = 4684: beyond the device's chirp-z sizes
+        dict(fs_out=9368e3, fc_out=0.0),                # n = 9368: beyond the device's chirp-z sizes
     ]
     plan = make_plan(fs, N, "s16le", filters, B, 5)
     assert plan.filter_status[:4] == [0, 0, 0, 0] and plan.filter_status[5] == 0
@@ -409,6 +409,7 @@ def test_carry_starts_mid_stream(fmt, mode):
 
 CHIRP_SIZES = [12, 20, 28, 36, 100, 300, 1000, 1012, 2340]
 CHIRP_SIZES_BIG = [3000, 4036, 4680]                    # chirp-z transforms of 8192 points
+CHIRP_SIZES_16K = [4684, 6000, 8188, 9000, 9364]        # 16384 points: their own kernel, any tile shape
 
 
 @pytest.mark.parametrize("fmt", ["s16le", "cf32le"])
@@ -420,7 +421,7 @@ def test_chirp_sizes_against_oracle(fmt, mode, shape):
     power-of-two channels in one plan, they meet the same bar."""
     N, B = 4096, 4
     cplx = oracle64.is_complex(fmt)
-    sizes = CHIRP_SIZES + (CHIRP_SIZES_BIG if shape[0] == 8192 else []) + [64, 8192]
+    sizes = CHIRP_SIZES + (CHIRP_SIZES_BIG if shape[0] == 8192 else []) + CHIRP_SIZES_16K + [64, 8192]
     filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * 4 * ((-1) ** i * (53 * i + 3) if cplx else 53 * i + 3))
                for i, n in enumerate(sizes)]
     plan = make_plan(N * 1000.0, N, fmt, filters, B, 3, mode=mode)
@@ -467,18 +468,21 @@ def test_split_limits():
 
 
 def test_chirp_limits():
-    """Sizes whose chirp-z transform exceeds 8192 points are dropped with a
-    status; a 4096-point tile shape is refused while a plan holds a chirp-z
-    size that needs 8192 points."""
+    """Sizes whose chirp-z transform exceeds 16384 points (n > 9364) are
+    dropped with a status; a 4096-point tile shape is refused while a plan
+    holds a chirp-z size that needs 8192 points, and allowed with the 16384-point
+    ones, which run in a kernel of their own."""
     N = 4096
-    filters = [dict(fs_out=1000.0 * n, fc_out=0.0) for n in (4680, 4684, 12)]
+    filters = [dict(fs_out=1000.0 * n, fc_out=0.0) for n in (4680, 9364, 9368, 12)]
     plan = make_plan(N * 1000.0, N, "s16le", filters, 4, 3)
-    assert plan.filter_status == [0, SK_ERR_UNSUPPORTED, 0]
-    assert [c["bins"] for c in plan.channels] == [4680, 12]
+    assert plan.filter_status == [0, 0, SK_ERR_UNSUPPORTED, 0]
+    assert [c["bins"] for c in plan.channels] == [4680, 9364, 12]
     with pytest.raises(SpektriError):
         plan.set_tuning(4096, 256, 1)
     plan.set_tuning(8192, 256, 1)
     assert plan.autotune("")[0] == 8192                          # no cache file
+    p16 = make_plan(N * 1000.0, N, "s16le", [filters[1], filters[3]], 4, 3)
+    p16.set_tuning(4096, 256, 4)
 
 
 def test_host_outputs_contiguous_and_separate():
