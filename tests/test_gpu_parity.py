@@ -372,6 +372,44 @@ def test_weights_update_and_custom_complex_weights():
     run_compare(plan, w.fmt, [r1], o64=o64)
 
 
+def test_time_shards_on_plans_reproduce_one_plan():
+    """The multi-GPU split (spektri_b200.shard) run with one Plan per shard on
+    this GPU, one after another: three shards of an 11-buffer stream, each
+    primed with the raw samples before it, give, concatenated in shard order,
+    the channel records and spectrum records (sequence numbers offset per
+    shard) of one plan over the whole stream, bit for bit."""
+    from spektri_b200 import shard
+    N, B, avg, nbuf, world = 2048, 4, 8, 11, 3
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * f) for n, f in ((64, 300), (512, 640), (2048, 100))]
+    rng = np.random.default_rng(23)
+    from tests.test_oracle import _stream
+    one = make_plan(N * 1000.0, N, "s16le", filters, B, avg)
+    raws = [_stream("s16le", one.new_samples, rng) for _ in range(nbuf)]
+    stream = np.concatenate([np.frombuffer(r, np.uint8) for r in raws])
+    full = [one.process(r) for r in raws]
+    shards = shard.plan_shards(nbuf, world, B, avg)
+    offs = shard.spectrum_seq_offsets(shards, B, avg)
+    assert [c for _, c in shards] == [4, 4, 3] and offs == [0, 2, 4]
+    bps = one.raw_bytes // one.new_samples
+    spectra, outs = [], []
+    for (first, count), off in zip(shards, offs):
+        p = make_plan(N * 1000.0, N, "s16le", filters, B, avg)
+        carry = shard.carry_bytes(stream, first, one.new_samples, one.overlap, bps)
+        if carry is not None:
+            p.set_carry(carry)
+        for b in range(first, first + count):
+            sp, oc = p.process(raws[b])
+            spectra += [(s + off, v) for s, v in sp]
+            outs.append(oc)
+        p.close()
+    assert [s for s, _ in spectra] == [s for f in full for s, _ in f[0]]
+    for (_, a), (_, r) in zip(spectra, [x for f in full for x in f[0]]):
+        assert np.array_equal(a, r)
+    for oc, f in zip(outs, full):
+        for a, r in zip(oc, f[1]):
+            assert np.array_equal(a, r)
+
+
 @pytest.mark.parametrize("fmt,mode", [("s16le", "batched"), ("cf32le", "plain"), ("u8", "batched")])
 def test_carry_starts_mid_stream(fmt, mode):
     """A plan primed with the N/4 samples before buffer k reproduces, bit for
