@@ -204,17 +204,73 @@ __global__ void __launch_bounds__(T, 2) fwd_fft_kernel(FwdArgs a) {
 }
 
 // Two-pass forward FFT for Nc = R1 * S with R1 >= 16 (Nc up to 2^21).
-// Pass A (columns): a tile holds C = S/R1 consecutive columns j2 of one block;
-// it loads z[j1 S + j2] row by row (coalesced), transposes into R1-point
-// transforms in shared memory, runs them, and stores
-// Y[k1][j2] = W_Nc^{j2 k1} sum_j1 z[j1 S + j2] W_R1^{j1 k1}.
+// Pass A (columns): a tile holds C = S/R1 consecutive columns j2 of one block
+// and computes Y[k1][j2] = W_Nc^{j2 k1} sum_j1 z[j1 S + j2] W_R1^{j1 k1} as
+// two decimation-in-time stages: radix 16 straight from the samples (thread
+// (col, q) loads z[(q + (R1/16) s) S + c0 + col], s < 16: lanes along
+// consecutive columns, so every load is coalesced), its outputs down the
+// column in shared memory (column stride R1 + 1, odd: conflict-free), then
+// radix R1/16 on span 16 whose outputs k1 = j + 16 u go straight to Y (lanes
+// along columns again, coalesced stores).  Shared memory is touched once each
+// way per element (R1 = 16 needs none).
 // Pass B (rows): S-point FFT of row k1 of Y gives Z[k1 + R1 k2], stored at
 // k1 S + k2 — the residue layout the spectrum split reads.
+template <int LOGR1, int T, int FMT>
+__device__ __forceinline__ void fwd_col_tile(float2* sm, const FwdArgs& a, const SampleSrc<FMT>& src, float2* Y) {
+  constexpr bool CPLX = (FMT & 0xC0) == 0x40;
+  constexpr int LOGS = TILE_LOGS, R1 = 1 << LOGR1, LOGC = LOGS - LOGR1, C = 1 << LOGC;
+  constexpr int LOGRB = LOGR1 - 4, RB = 1 << LOGRB, ROW = R1 + 1;
+  static_assert(C * (R1 / 16) == T, "one radix-16 butterfly per thread");
+  const int b = blockIdx.x >> LOGR1;
+  const int c0 = (blockIdx.x & (R1 - 1)) << LOGC;
+  const long long p0 = (long long)b * a.hop;
+  const int shC = a.log2N - a.log2Nc;
+  float2* Yb = Y + ((size_t)b << a.log2Nc) + c0;
+  const int col = threadIdx.x & (C - 1), q = threadIdx.x >> LOGC;
+  float2 v[16];
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const int jj = ((q + (s << LOGRB)) << LOGS) + c0 + col;
+    const float2 z = src.pair(p0 + (CPLX ? jj : 2 * jj));
+    v[s] = make_float2(z.x * a.wscale, z.y * a.wscale);
+  }
+  dft<16, -1>(v);
+  if constexpr (RB == 1) {                                  // R1 = 16: k1 = u
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const float2 t = u ? cmul(v[u], __ldg(&a.tw_big[((c0 + col) * u) << shC])) : v[u];
+      Yb[((size_t)u << LOGS) + col] = t;
+    }
+  } else {
+    float2* p = sm + col * ROW + q * 16;                     // Stockham: y[q 16 + u]
+#pragma unroll
+    for (int u = 0; u < 16; ++u) p[u] = v[u];
+    __syncthreads();
+    constexpr int NB = 16 * C / T;                           // radix-RB butterflies per thread
+#pragma unroll
+    for (int bb = 0; bb < NB; ++bb) {
+      const int beta = threadIdx.x + bb * T;
+      const int cl = beta & (C - 1), j = beta >> LOGC;       // column, span-16 index
+      const float2* r = sm + cl * ROW + j;
+      float2 w[RB];
+#pragma unroll
+      for (int s = 0; s < RB; ++s) w[s] = r[16 * s];
+      twiddle_dft<RB, TILE_LOGS - LOGR1, -1>(w, a.tw_tile, j);   // W_R1^(j s), span 16
+#pragma unroll
+      for (int u = 0; u < RB; ++u) {
+        const int k1 = j + 16 * u;
+        const float2 t = k1 ? cmul(w[u], __ldg(&a.tw_big[((c0 + cl) * k1) << shC])) : w[u];
+        Yb[((size_t)k1 << LOGS) + cl] = t;
+      }
+    }
+  }
+}
+
 template <int S, int T, int FMT>
-__global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {   // T = 512: 16 elements per thread
+__global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {   // T = 512
   extern __shared__ float2 sm[];
   constexpr bool CPLX = (FMT & 0xC0) == 0x40;
-  constexpr int E = S / T, LOGS = ilog2c(S);
+  static_assert(S == TILE_S && T == 512, "8192-point column tiles of 512 threads");
   trace_start(a.trace, 0);
   reset_cursors(a.cursor);
   const SampleSrc<FMT> src{a.raw, a.halo, a.overlap};
@@ -225,37 +281,12 @@ __global__ void __launch_bounds__(T, 2) fwd_col_kernel(FwdArgs a, float2* Y) {  
     for (long long h = (long long)blockIdx.x * T + threadIdx.x; h < ncomp; h += stride)
       a.halo_next[h] = load_comp<FMT & 0x3F>(a.raw, base + h);
   }
-  const int LOGR1 = a.log2R1, R1 = 1 << LOGR1, LOGC = LOGS - LOGR1, C = 1 << LOGC;
-  const PadCols pad{LOGR1};                                 // consecutive threads write consecutive columns
-  const int b = blockIdx.x >> LOGR1;
-  const int c0 = (blockIdx.x & (R1 - 1)) << LOGC;
-  const long long p0 = (long long)b * a.hop;
-#pragma unroll 4
-  for (int k = 0; k < E; ++k) {
-    const int g = threadIdx.x + k * T;
-    const int j1 = g >> LOGC, col = g & (C - 1);
-    const int jj = (j1 << LOGS) + c0 + col;
-    const float2 z = src.pair(p0 + (CPLX ? jj : 2 * jj));
-    sm[pad((col << LOGR1) + j1)] = make_float2(z.x * a.wscale, z.y * a.wscale);
-  }
-  __syncthreads();
-  switch (LOGR1) {                                          // R1-point column transforms, in place
-    case 4: tile_fft_inplace<4, S, T, -1>(sm, a.tw_tile, pad); break;
-    case 5: tile_fft_inplace<5, S, T, -1>(sm, a.tw_tile, pad); break;
-    case 6: tile_fft_inplace<6, S, T, -1>(sm, a.tw_tile, pad); break;
-    case 7: tile_fft_inplace<7, S, T, -1>(sm, a.tw_tile, pad); break;
-    case 8: tile_fft_inplace<8, S, T, -1>(sm, a.tw_tile, pad); break;
-  }
-  __syncthreads();
-  const int shC = a.log2N - a.log2Nc;
-  float2* Yb = Y + ((size_t)b << a.log2Nc);
-#pragma unroll 4
-  for (int k = 0; k < E; ++k) {
-    const int g = threadIdx.x + k * T;
-    const int k1 = g >> LOGC, col = g & (C - 1);
-    float2 v = sm[pad((col << LOGR1) + k1)];
-    if (k1) v = cmul(v, __ldg(&a.tw_big[((c0 + col) * k1) << shC]));
-    Yb[((size_t)k1 << LOGS) + c0 + col] = v;
+  switch (a.log2R1) {
+    case 4: fwd_col_tile<4, T, FMT>(sm, a, src, Y); break;
+    case 5: fwd_col_tile<5, T, FMT>(sm, a, src, Y); break;
+    case 6: fwd_col_tile<6, T, FMT>(sm, a, src, Y); break;
+    case 7: fwd_col_tile<7, T, FMT>(sm, a, src, Y); break;
+    case 8: fwd_col_tile<8, T, FMT>(sm, a, src, Y); break;
   }
 }
 
