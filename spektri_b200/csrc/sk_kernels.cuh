@@ -247,20 +247,36 @@ __device__ __forceinline__ void fwd_col_tile(float2* sm, const FwdArgs& a, const
     for (int u = 0; u < 16; ++u) p[u] = v[u];
     __syncthreads();
     constexpr int NB = 16 * C / T;                           // radix-RB butterflies per thread
+    static_assert(C <= T, "a thread's butterflies share one column");
+    // Output k1 = j + 16 u of column j2 = c0 + cl takes W_Nc^(j2 k1) =
+    // W_Nc^(j2 j) (w16)^u, w16 = W_Nc^(16 j2): one gathered table read per
+    // butterfly, the powers of w16 from w16 and w16^4 (as TwiddlePowers does)
+    const int cl = threadIdx.x & (C - 1), j2 = c0 + cl;
+    float2 pw[4] = {make_float2(1.f, 0.f), __ldg(&a.tw_big[(16 * j2) << shC]), {}, {}};
+    pw[2] = cmul(pw[1], pw[1]);
+    pw[3] = cmul(pw[2], pw[1]);
+    float2 m[4] = {make_float2(1.f, 0.f), {}, {}, {}};
+    if constexpr (RB > 4) {
+      m[1] = __ldg(&a.tw_big[(64 * j2) << shC]);
+      m[2] = cmul(m[1], m[1]);
+      m[3] = cmul(m[2], m[1]);
+    }
 #pragma unroll
     for (int bb = 0; bb < NB; ++bb) {
-      const int beta = threadIdx.x + bb * T;
-      const int cl = beta & (C - 1), j = beta >> LOGC;       // column, span-16 index
+      const int j = (threadIdx.x + bb * T) >> LOGC;          // span-16 index
       const float2* r = sm + cl * ROW + j;
       float2 w[RB];
 #pragma unroll
       for (int s = 0; s < RB; ++s) w[s] = r[16 * s];
       twiddle_dft<RB, TILE_LOGS - LOGR1, -1>(w, a.tw_tile, j);   // W_R1^(j s), span 16
+      const float2 base = __ldg(&a.tw_big[(j2 * j) << shC]);
 #pragma unroll
       for (int u = 0; u < RB; ++u) {
         const int k1 = j + 16 * u;
-        const float2 t = k1 ? cmul(w[u], __ldg(&a.tw_big[((c0 + cl) * k1) << shC])) : w[u];
-        Yb[((size_t)k1 << LOGS) + cl] = t;
+        float2 tw = (u & 3) ? pw[u & 3] : m[u >> 2];
+        if ((u & 3) && (u >> 2)) tw = cmul(tw, m[u >> 2]);
+        tw = u ? cmul(base, tw) : base;
+        Yb[((size_t)k1 << LOGS) + cl] = k1 ? cmul(w[u], tw) : w[u];
       }
     }
   }
