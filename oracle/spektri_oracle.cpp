@@ -54,6 +54,8 @@ struct FftPlan {
   std::vector<int> radices;
   std::vector<std::vector<cf>> tw;   // per stage: [s-1][j], s in 1..R-1, j in 0..L-1
   std::vector<std::vector<cf>> wr;   // per stage: W_R^k for generic radices
+  std::vector<std::vector<float>> twr, twi;   // the same twiddles split into real and imaginary parts
+  bool soa = false;                  // every radix 4 or 2: the structure-of-arrays path
 
   FftPlan() {}
   FftPlan(int n_, int sign_) : n(n_), sign(sign_) {
@@ -77,13 +79,110 @@ struct FftPlan {
         w[k] = {(float)std::cos(a), (float)std::sin(a)};
       }
       wr.push_back(std::move(w));
+      std::vector<float> tr(tw.back().size()), ti(tw.back().size());
+      for (size_t k = 0; k < tr.size(); ++k) { tr[k] = tw.back()[k].re; ti[k] = tw.back()[k].im; }
+      twr.push_back(std::move(tr));
+      twi.push_back(std::move(ti));
       L *= R;
     }
+    soa = n > 1;
+    for (int R : radices) soa = soa && (R == 4 || R == 2);
+  }
+
+  // One radix-4 (R = 4) or radix-2 stage of span L on split real/imaginary
+  // arrays, with exactly the arithmetic of the generic butterfly below (the
+  // same products and sums in the same order, so the same bits); for L >= 8
+  // the inner loop runs along j, contiguous on both sides, which the compiler
+  // vectorises.
+  template <int R, int SIGN>
+  static inline void bfly_soa(int q, int o, int j, int L, int stride, const float* __restrict__ sr,
+                              const float* __restrict__ si, float* __restrict__ dr, float* __restrict__ di,
+                              const float* __restrict__ tr, const float* __restrict__ ti) {
+    const float x0r = sr[q], x0i = si[q];
+    if (R == 2) {
+      const float ar = sr[q + stride], ai = si[q + stride], wr_ = tr[j], wi_ = ti[j];
+      const float x1r = ar * wr_ - ai * wi_, x1i = ar * wi_ + ai * wr_;
+      dr[o] = x0r + x1r; di[o] = x0i + x1i;
+      dr[o + L] = x0r - x1r; di[o + L] = x0i - x1i;
+    } else {
+      const float a1r = sr[q + stride], a1i = si[q + stride];
+      const float a2r = sr[q + 2 * stride], a2i = si[q + 2 * stride];
+      const float a3r = sr[q + 3 * stride], a3i = si[q + 3 * stride];
+      const float w1r = tr[j], w1i = ti[j], w2r = tr[L + j], w2i = ti[L + j], w3r = tr[2 * L + j], w3i = ti[2 * L + j];
+      const float x1r = a1r * w1r - a1i * w1i, x1i = a1r * w1i + a1i * w1r;
+      const float x2r = a2r * w2r - a2i * w2i, x2i = a2r * w2i + a2i * w2r;
+      const float x3r = a3r * w3r - a3i * w3i, x3i = a3r * w3i + a3i * w3r;
+      const float s02r = x0r + x2r, s02i = x0i + x2i, d02r = x0r - x2r, d02i = x0i - x2i;
+      const float s13r = x1r + x3r, s13i = x1i + x3i, d13r = x1r - x3r, d13i = x1i - x3i;
+      const float r13r = SIGN < 0 ? d13i : -d13i, r13i = SIGN < 0 ? -d13r : d13r;   // d13 * (sign i)
+      dr[o] = s02r + s13r;         di[o] = s02i + s13i;
+      dr[o + L] = d02r + r13r;     di[o + L] = d02i + r13i;
+      dr[o + 2 * L] = s02r - s13r; di[o + 2 * L] = s02i - s13i;
+      dr[o + 3 * L] = d02r - r13r; di[o + 3 * L] = d02i - r13i;
+    }
+  }
+
+  // One radix-4 (R = 4) or radix-2 stage of span L on split real/imaginary
+  // arrays, with exactly the arithmetic of the generic butterfly below (the
+  // same products and sums in the same order, so the same bits); for L >= 8
+  // the inner loop runs along j, contiguous on both sides, which the compiler
+  // vectorises.
+  template <int R, int SIGN>
+  void stage_soa(int st, int L, const float* __restrict__ sr, const float* __restrict__ si, float* __restrict__ dr,
+                 float* __restrict__ di) const {
+    const int stride = n / R, groups = n / (L * R);
+    const float* __restrict__ tr = twr[st].data();
+    const float* __restrict__ ti = twi[st].data();
+    if (L >= 8) {
+      for (int g = 0; g < groups; ++g) {
+        const float* __restrict__ s0r = sr + g * L;
+        const float* __restrict__ s0i = si + g * L;
+        float* __restrict__ d0r = dr + g * L * R;
+        float* __restrict__ d0i = di + g * L * R;
+#pragma GCC ivdep
+        for (int j = 0; j < L; ++j) bfly_soa<R, SIGN>(j, j, j, L, stride, s0r, s0i, d0r, d0i, tr, ti);
+      }
+    } else if (L == 1) {
+      stage_short<R, SIGN, 1>(groups, stride, sr, si, dr, di, tr, ti);
+    } else if (L == 2) {
+      stage_short<R, SIGN, 2>(groups, stride, sr, si, dr, di, tr, ti);
+    } else {
+      stage_short<R, SIGN, 4>(groups, stride, sr, si, dr, di, tr, ti);
+    }
+  }
+
+  // Short spans (L = 1, 2, 4) with L a compile-time constant, so the loop over
+  // groups has constant strides (interleaved stores the compiler can vectorise).
+  template <int R, int SIGN, int LC>
+  static void stage_short(int groups, int stride, const float* __restrict__ sr, const float* __restrict__ si,
+                          float* __restrict__ dr, float* __restrict__ di, const float* __restrict__ tr,
+                          const float* __restrict__ ti) {
+#pragma GCC ivdep
+    for (int g = 0; g < groups; ++g)
+      for (int j = 0; j < LC; ++j) bfly_soa<R, SIGN>(g * LC + j, g * LC * R + j, j, LC, stride, sr, si, dr, di, tr, ti);
+  }
+
+  void run_soa(cf* x) const {
+    thread_local std::vector<float> buf;
+    if (buf.size() < 4 * (size_t)n) buf.resize(4 * (size_t)n);
+    float *ar = buf.data(), *ai = ar + n, *br = ai + n, *bi = br + n;
+    for (int k = 0; k < n; ++k) { ar[k] = x[k].re; ai[k] = x[k].im; }
+    int L = 1;
+    for (size_t st = 0; st < radices.size(); ++st) {
+      const int R = radices[st];
+      if (R == 4) { if (sign < 0) stage_soa<4, -1>((int)st, L, ar, ai, br, bi); else stage_soa<4, 1>((int)st, L, ar, ai, br, bi); }
+      else        { if (sign < 0) stage_soa<2, -1>((int)st, L, ar, ai, br, bi); else stage_soa<2, 1>((int)st, L, ar, ai, br, bi); }
+      std::swap(ar, br);
+      std::swap(ai, bi);
+      L *= R;
+    }
+    for (int k = 0; k < n; ++k) x[k] = {ar[k], ai[k]};
   }
 
   // In place on x (n values) using scratch y (n values).
   void run(cf* x, cf* y) const {
     if (n <= 1) return;
+    if (soa) { run_soa(x); return; }
     cf* src = x; cf* dst = y;
     int L = 1;
     for (size_t st = 0; st < radices.size(); ++st) {
@@ -263,7 +362,13 @@ struct orc_filter {
   int32_t transition;        // >0 and weights NULL: Tukey with that taper width
 };
 
-struct Chan { long long bins, first; std::vector<cf> w; FftPlan ifft; };
+struct Chan {
+  long long bins, first;
+  std::vector<cf> w;
+  FftPlan ifft;
+  std::vector<long long> gi;   // get_bin's modulo and mirror (fftutil.rs:8-22) for IFFT input i:
+  std::vector<uint8_t> gc;     // spectrum index and whether to conjugate
+};
 
 struct orc_state {
   orc_params p;
@@ -317,6 +422,14 @@ orc_state* orc_create(const orc_params* p, const orc_filter* f, int32_t nf, int3
       c.w = raised_cosine((int)bins);
     }
     c.ifft = FftPlan((int)bins, +1);
+    const long long shift = bins / 2, NN = s->N, KK = s->K;
+    c.gi.resize(bins);
+    c.gc.resize(bins);
+    for (long long i = 0; i < (long long)bins; ++i) {
+      const long long m = (((c.first + (i + shift) % bins) % NN) + NN) % NN;
+      c.gi[i] = m < KK ? m : NN - m;
+      c.gc[i] = m < KK ? 0 : 1;
+    }
     s->ch.push_back(std::move(c));
   }
   return s;
@@ -351,14 +464,20 @@ int32_t orc_process(orc_state* s, const uint8_t* raw, float* const* chan_out, vo
   const int fmt = s->p.input_format, nth = std::max(1, s->p.n_threads);
   const int bps = fmt_bytes(fmt);
   // main.rs:173 then main.rs:181
+  const long long nchunk = 64, chunk = (s->nnew + nchunk - 1) / nchunk;
   if (s->cplx) {
     std::memmove(s->cbuf.data(), s->cbuf.data() + s->nnew, sizeof(cf) * s->overlap);
     int half = bps / 2;
-    for (long long i = 0; i < s->nnew; ++i)
-      s->cbuf[s->overlap + i] = {conv1(raw + i * bps, fmt), conv1(raw + i * bps + half, fmt)};
+    parallel_for((int)nchunk, nth, [&](int c) {
+      for (long long i = c * chunk; i < std::min(s->nnew, (c + 1) * chunk); ++i)
+        s->cbuf[s->overlap + i] = {conv1(raw + i * bps, fmt), conv1(raw + i * bps + half, fmt)};
+    });
   } else {
     std::memmove(s->rbuf.data(), s->rbuf.data() + s->nnew, sizeof(float) * s->overlap);
-    for (long long i = 0; i < s->nnew; ++i) s->rbuf[s->overlap + i] = conv1(raw + i * bps, fmt);
+    parallel_for((int)nchunk, nth, [&](int c) {
+      for (long long i = c * chunk; i < std::min(s->nnew, (c + 1) * chunk); ++i)
+        s->rbuf[s->overlap + i] = conv1(raw + i * bps, fmt);
+    });
   }
   const float w = s->window;
   // multifft.rs:34-95
@@ -386,70 +505,89 @@ int32_t orc_process(orc_state* s, const uint8_t* raw, float* const* chan_out, vo
       }
     });
   }
-  // spectrum.rs:82-163
-  int ns = 0;
+  // spectrum.rs:82-163.  Records complete at fixed blocks of the buffer, so
+  // the bins run in parallel ranges, each bin's terms summed in block order
+  // (the same additions as a loop over blocks outside, bins inside).
   if (spec_seq0) *spec_seq0 = s->spec_seq;
   const int sb = spec_bytes(s->p.spectrum_format);
-  for (long long b = 0; b < B; ++b) {
-    const cf* Xb = s->X.data() + (size_t)b * K;
-    float* acc = s->acc.data();
-    const long long edges[2] = {0, K - 1};
-    for (long long e : edges) {
-      cf c0 = get_bin(Xb, N, K, e), cm = get_bin(Xb, N, K, e - 1), cp = get_bin(Xb, N, K, e + 1);
-      cf c = {c0.re - (cm.re + cp.re) * 0.5f, c0.im - (cm.im + cp.im) * 0.5f};
-      acc[e] += c.re * c.re + c.im * c.im;
-      if (K == 1) break;
-    }
-    for (long long k = 1; k + 1 < K; ++k) {
-      cf c = {Xb[k].re - (Xb[k - 1].re + Xb[k + 1].re) * 0.5f, Xb[k].im - (Xb[k - 1].im + Xb[k + 1].im) * 0.5f};
-      acc[k] += c.re * c.re + c.im * c.im;
-    }
-    s->accn += 1;
-    if (s->accn >= (uint32_t)s->p.averages) {
-      uint8_t* out = (uint8_t*)spec_out + (size_t)ns * K * sb;
-      float db_plus = std::log10((float)s->accn) * -10.0f;
-      for (long long k = 0; k < K; ++k) {
-        if (s->p.spectrum_format == 2) {
-          float v = acc[k] / (float)s->accn;
-          std::memcpy(out + 4 * k, &v, 4);
-          continue;
-        }
-        float db = std::log10(acc[k]) * 10.0f + db_plus;
-        if (s->p.spectrum_format == 1) {
-          float q = std::fmin(std::fmax(db * 20.0f + 4000.0f, 0.0f), 4095.0f);   // fmax(NaN,0)=0 like f32::max
-          uint16_t o = (uint16_t)q;
-          out[2 * k] = (uint8_t)(o >> 8); out[2 * k + 1] = (uint8_t)(o & 0xFF);
-        } else {
-          float q = std::fmin(std::fmax(db * 2.0f + 250.0f, 0.0f), 255.0f);
-          out[k] = (uint8_t)q;
+  std::vector<long long> emit_at;                  // blocks after which a record completes
+  {
+    uint32_t a = s->accn;
+    for (long long b = 0; b < B; ++b)
+      if (++a >= (uint32_t)s->p.averages) { emit_at.push_back(b); a = 0; }
+  }
+  const uint32_t accn0 = s->accn;
+  const long long kchunk = 4096, nk = (K + kchunk - 1) / kchunk;
+  parallel_for((int)nk, nth, [&](int kc) {
+    const long long k0 = kc * kchunk, k1 = std::min(K, k0 + kchunk);
+    for (long long k = k0; k < k1; ++k) {
+      float a = s->acc[k];
+      uint32_t cnt = accn0;
+      int r = 0;
+      const bool edge = k == 0 || k == K - 1;
+      for (long long b = 0; b < B; ++b) {
+        const cf* Xb = s->X.data() + (size_t)b * K;
+        cf c0, cm, cp;
+        if (edge) { c0 = get_bin(Xb, N, K, k); cm = get_bin(Xb, N, K, k - 1); cp = get_bin(Xb, N, K, k + 1); }
+        else { c0 = Xb[k]; cm = Xb[k - 1]; cp = Xb[k + 1]; }
+        cf c = {c0.re - (cm.re + cp.re) * 0.5f, c0.im - (cm.im + cp.im) * 0.5f};
+        a += c.re * c.re + c.im * c.im;
+        if (++cnt >= (uint32_t)s->p.averages) {
+          uint8_t* out = (uint8_t*)spec_out + (size_t)r * K * sb;
+          if (s->p.spectrum_format == 2) {
+            float v = a / (float)cnt;
+            std::memcpy(out + 4 * k, &v, 4);
+          } else {
+            float db_plus = std::log10((float)cnt) * -10.0f;
+            float db = std::log10(a) * 10.0f + db_plus;
+            if (s->p.spectrum_format == 1) {
+              float q = std::fmin(std::fmax(db * 20.0f + 4000.0f, 0.0f), 4095.0f);   // fmax(NaN,0)=0 like f32::max
+              uint16_t o = (uint16_t)q;
+              out[2 * k] = (uint8_t)(o >> 8); out[2 * k + 1] = (uint8_t)(o & 0xFF);
+            } else {
+              float q = std::fmin(std::fmax(db * 2.0f + 250.0f, 0.0f), 255.0f);
+              out[k] = (uint8_t)q;
+            }
+          }
+          a = 0.0f;
+          cnt = 0;
+          ++r;
         }
       }
-      std::fill(s->acc.begin(), s->acc.end(), 0.0f);
-      s->accn = 0;
-      s->spec_seq += 1;
-      ns += 1;
+      s->acc[k] = a;
     }
-  }
+  });
+  const int ns = (int)emit_at.size();
+  s->accn = emit_at.empty() ? accn0 + (uint32_t)B : (uint32_t)(B - 1 - emit_at.back());
+  s->spec_seq += ns;
   if (n_spec) *n_spec = ns;
-  // fcfb.rs:66-100 / 154-188
-  parallel_for((int)s->ch.size(), nth, [&](int ci) {
+  // fcfb.rs:66-100 / 154-188.  Work items of (channel, run of blocks), the
+  // largest IFFT sizes first, so that threads finish together.
+  constexpr long long BRUN = 8;
+  std::vector<std::pair<int, long long>> items;
+  for (size_t ci = 0; ci < s->ch.size(); ++ci)
+    for (long long b0 = 0; b0 < B; b0 += BRUN) items.push_back({(int)ci, b0});
+  std::stable_sort(items.begin(), items.end(), [&](const auto& x, const auto& y) {
+    return s->ch[x.first].bins > s->ch[y.first].bins;
+  });
+  parallel_for((int)items.size(), nth, [&](int it) {
+    const int ci = items[it].first;
     const Chan& c = s->ch[ci];
-    const long long n = c.bins, shift = n / 2;
-    std::vector<cf> buf(n), y(n);
-    float* dst = chan_out ? chan_out[ci] : nullptr;
-    for (long long b = 0; b < B; ++b) {
+    const long long n = c.bins, shift = n / 2, keep = n / 8 * 6;
+    thread_local std::vector<cf> buf, y;
+    if ((long long)buf.size() < n) { buf.resize(n); y.resize(n); }
+    const long long b1 = std::min(B, items[it].second + BRUN);
+    for (long long b = items[it].second; b < b1; ++b) {
       const cf* Xb = s->X.data() + (size_t)b * K;
       for (long long i = 0; i < n; ++i) {
-        long long j = (i + shift) % n;
-        cf v = get_bin(Xb, N, K, c.first + j);
+        const long long j = i + shift < n ? i + shift : i + shift - n;
+        cf v = Xb[c.gi[i]];
+        if (c.gc[i]) v.im = -v.im;
         cf wj = c.w[j];
         buf[i] = (wj.im == 0.0f) ? cf{wj.re * v.re, wj.re * v.im} : cmul(wj, v);
       }
       c.ifft.run(buf.data(), y.data());
-      if (dst) {
-        std::memcpy(dst, buf.data() + n / 8, sizeof(cf) * (size_t)(n / 8 * 6));
-        dst += 2 * (n / 8 * 6);
-      }
+      if (chan_out) std::memcpy(chan_out[ci] + 2 * b * keep, buf.data() + n / 8, sizeof(cf) * (size_t)keep);
     }
   });
   return 0;
