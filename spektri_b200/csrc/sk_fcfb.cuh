@@ -280,29 +280,6 @@ __device__ __forceinline__ void tile_chirp(float2* sm, int count, const float2* 
   }
 }
 
-// Every 2^LOGN-point transform of the tile, already in shared memory (index
-// policy pad), transformed in place: each stage reads all its inputs, syncs,
-// writes; the caller syncs before and after.
-template <int LOGN, int S, int T, int DIR, class Pad>
-__device__ __forceinline__ void tile_fft_inplace(float2* sm, const float2* __restrict__ tw, const Pad& pad) {
-  using P = StagePlan<LOGN, S / T>;
-  constexpr int count = S >> LOGN;
-  auto none = [](int, int, int, float2) {};
-  stage_next<LOGN, 1 << P::r0, 0, S, T, DIR, false>(sm, count, tw, none, pad);
-  if constexpr (P::ns >= 2) {
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, none, pad);
-  }
-  if constexpr (P::ns >= 3) {
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, none, pad);
-  }
-  if constexpr (P::ns >= 4) {
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, false>(sm, count, tw, none, pad);
-  }
-}
-
 // ------------------------------------------------------------------ filter bank
 // The filter bank reads the spectra in an extended layout: per block a row of
 // xs >= N + maxn bins holding get_bin(X, N, m) (fftutil.rs:8-22) at every

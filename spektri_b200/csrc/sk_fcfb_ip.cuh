@@ -39,9 +39,6 @@ struct IpPlan {
   static constexpr int n = 1 << LOGN, NL = n >> 4, ROW = NL + 1, SPAN = n + 16;
 };
 
-// Shared-memory elements a tile of S points needs (S/n transforms of n + 16).
-constexpr int ip_smem_elems(int S) { return S + 16 * (S >> 9); }
-
 // load(t, q, s): input i = q + NL s of transform t.  store(t, kk, u, v):
 // output o = kk + (n/R1) u (the Stockham stores' convention).  count
 // transforms (t < count); the caller syncs before (shared memory free).
@@ -137,7 +134,7 @@ __device__ __forceinline__ void fcfb_tile_ip(float2* sm, const TileMeta* meta, i
 // last stage (odd stride 513), consecutive q in the leaf.  DIR = +1 is the
 // inverse transform (the filter bank), -1 the forward one (the row pass of
 // the two-pass forward FFT).
-constexpr int IP8K_ROW = 513, IP8K_SPAN = 8192 + 16;
+constexpr int IP8K_ROW = 513;                // 8192 + 16 elements of shared memory
 
 template <int T, int DIR = +1, class Load, class Store>
 __device__ __forceinline__ void ip_pipeline_8k(float2* sm, const float2* __restrict__ tw, Load& load, Store& store) {

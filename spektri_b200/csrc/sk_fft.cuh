@@ -1,8 +1,6 @@
-// FP32 FFT building blocks for sm_100a: complex helpers, in-register DFTs of
-// 2..32 points, and the shared-memory "tile" engine that runs S/n independent
-// n-point transforms (n a power of two, 4 <= n <= S) with T threads.
-//
-// Tile engine (Stockham autosort, decimation in time).  A stage of radix R on
+// FP32 FFT building blocks for sm_100a: complex helpers and in-register DFTs
+// of 2..32 points, used by the tile pipelines (sk_fcfb.cuh: Stockham stages;
+// sk_fcfb_ip.cuh: in-place stages).  A Stockham stage of radix R on
 // sub-transforms of span L maps, inside each n-point transform,
 //   q in [0, n/R):  j = q mod L,  g = q div L,
 //   a_s = x[q + s n/R] * W_{LR}^{j s}            (s = 0..R-1)
@@ -135,106 +133,10 @@ struct DftLeaf<2, DIR, STRIDE, OFF> {
 // Shared-memory index with one pad slot per 16 float2: radix-R scatters at
 // stride R (R <= 16) then land in distinct 8-byte banks of a half warp.
 __device__ __forceinline__ int padx(int a) { return a + (a >> 4); }
-template <int S>
-struct TileShape {
-  static constexpr int LOGS = ilog2c(S);
-  static constexpr int SMEM_ELEMS = S + S / 16;
-  static constexpr size_t SMEM_BYTES = sizeof(float2) * (size_t)SMEM_ELEMS;
-};
 
-// Shared-memory index policies: padx, and padx plus one slot per transform
-// (for tiles written column-wise, one transform per column: with 2^logn-point
-// transforms the column stride n + n/16 + 1 is odd in 8-byte slots for
-// n >= 32, so a warp writing 32 consecutive columns hits every bank pair).
+// Shared-memory index policy of the Stockham stages (sk_fcfb.cuh).
 struct PadX {
   __device__ __forceinline__ int operator()(int e) const { return padx(e); }
 };
-struct PadCols {
-  int logn;
-  __device__ __forceinline__ int operator()(int e) const { return padx(e) + (e >> logn); }
-};
-
-// One Stockham stage of radix R over the whole tile (S/n transforms).
-// Reads, sync, writes, sync: the caller syncs before the first stage.
-// tw: forward table W_S^k, k in [0, S).
-template <int R, int DIR, int S, int T, class Pad = PadX>
-__device__ __forceinline__ void tile_stage(float2* sm, const float2* __restrict__ tw, int log2n, int log2L,
-                                           const Pad& pad = Pad()) {
-  constexpr int NB = S / (R * T);
-  static_assert(NB >= 1, "radix larger than elements per thread");
-  constexpr int LOGR = ilog2c(R);
-  constexpr int LOGS = ilog2c(S);
-  const int log2nR = log2n - LOGR;
-  float2 v[NB][R];
-  int ob[NB];
-#pragma unroll
-  for (int bb = 0; bb < NB; ++bb) {
-    const int beta = threadIdx.x + bb * T;
-    const int t = beta >> log2nR;
-    const int q = beta & ((1 << log2nR) - 1);
-    const int j = q & ((1 << log2L) - 1);
-    const int g = q >> log2L;
-    const int base = t << log2n;
-#pragma unroll
-    for (int s = 0; s < R; ++s) v[bb][s] = sm[pad(base + q + (s << log2nR))];
-    if (log2L > 0) {
-      const int sh = LOGS - log2L - LOGR;       // S / (L R) = 2^sh
-#pragma unroll
-      for (int s = 1; s < R; ++s) {
-        float2 w = __ldg(&tw[(j * s) << sh]);
-        if (DIR > 0) w.y = -w.y;
-        v[bb][s] = cmul(v[bb][s], w);
-      }
-    }
-    dft<R, DIR>(v[bb]);
-    ob[bb] = base + (g << (log2L + LOGR)) + j;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int bb = 0; bb < NB; ++bb) {
-#pragma unroll
-    for (int u = 0; u < R; ++u) sm[pad(ob[bb] + (u << log2L))] = v[bb][u];
-  }
-  __syncthreads();
-}
-
-// log2 of the radix of stage p for a 2^log2n-point transform (0 = no stage).
-__device__ __forceinline__ int stage_radix(int log2n, int p) {
-  // 4:[4] 8:[8] 16:[16] 32:[32] 64:[8,8] 128:[16,8] 256:[16,16] 512:[16,32]
-  // 1024:[32,32] 2048:[16,16,8] 4096:[16,16,16] 8192:[16,16,32]
-  switch (log2n) {
-    case 2: return p == 0 ? 2 : 0;
-    case 3: return p == 0 ? 3 : 0;
-    case 4: return p == 0 ? 4 : 0;
-    case 5: return p == 0 ? 5 : 0;
-    case 6: return p < 2 ? 3 : 0;
-    case 7: return p == 0 ? 4 : p == 1 ? 3 : 0;
-    case 8: return p < 2 ? 4 : 0;
-    case 9: return p == 0 ? 4 : p == 1 ? 5 : 0;
-    case 10: return p < 2 ? 5 : 0;
-    case 11: return p < 2 ? 4 : p == 2 ? 3 : 0;
-    case 12: return p < 3 ? 4 : 0;
-    case 13: return p < 2 ? 4 : p == 2 ? 5 : 0;
-  }
-  return 0;
-}
-
-// All stages of a batched 2^log2n-point FFT over the tile in shared memory.
-template <int DIR, int S, int T, class Pad = PadX>
-__device__ __forceinline__ void tile_fft(float2* sm, const float2* __restrict__ tw, int log2n, const Pad& pad = Pad()) {
-  int log2L = 0;
-#pragma unroll 1
-  for (int p = 0; p < 3; ++p) {
-    const int lr = stage_radix(log2n, p);
-    if (lr == 0) break;
-    switch (lr) {
-      case 2: tile_stage<4, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
-      case 3: tile_stage<8, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
-      case 4: tile_stage<16, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
-      case 5: tile_stage<32, DIR, S, T>(sm, tw, log2n, log2L, pad); break;
-    }
-    log2L += lr;
-  }
-}
 
 }  // namespace sk
