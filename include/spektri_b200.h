@@ -146,7 +146,12 @@ const char* sk_version(void);
 
 /* ------------------------------------------------------------ plans
  * DspState::init + Fcfb::add_filter per filter.  filter_status (optional,
- * n_filters entries) receives SK_OK or the reason each filter was dropped. */
+ * n_filters entries) receives SK_OK or the reason each filter was dropped.
+ * Sizes: fft_size a power of two (8 .. 2^21 complex points, 2^22 real
+ * samples) or 3 * 2^k, 5 * 2^k whose complex length is R1 M with R1 = 3, 5,
+ * 6, 10 or 12 and M = 16 .. 8192, else SK_ERR_UNSUPPORTED; filter IFFT sizes powers of
+ * two from 4 to 65536 or other multiples of 4 up to 9364 (chirp-z), others
+ * dropped with SK_ERR_UNSUPPORTED in filter_status. */
 int sk_plan_create(const sk_params* params, const sk_filter* filters, int32_t n_filters,
                    int32_t* filter_status, sk_plan** out);
 int sk_plan_info_get(const sk_plan* plan, sk_plan_info* info);
