@@ -185,6 +185,24 @@ def test_c3_shape_plain_equals_batched_and_oracle():
         assert max(errs) < TOL, max(errs)
 
 
+@pytest.mark.parametrize("spec", ["f32", "u8", "u16"])
+def test_two_pass_complex_welch_records(spec):
+    """Complex input through the two-pass FFT with 16 residue rows (N = 2^17,
+    the transposing Welch kernel): 6 blocks per buffer and 4 averages, so
+    records complete mid-buffer and the accumulator carries across buffers;
+    f32 records within 1e-5 of FP64, u8/u16 codes within 1 LSB, channel
+    outputs within 1e-5 (edge channels wrap past bin 0 and N - 1)."""
+    N, B = 1 << 17, 6
+    fs = N * 1000.0
+    filters = [dict(fs_out=1000.0 * n, fc_out=1000.0 * f) for n, f in
+               ((256, 0.0), (1024, -65536 + 8), (4096, 12340), (64, 65532))]
+    plan = make_plan(fs, N, "cs16le", filters, B, 4, spec=spec)
+    assert plan.n_channels == 4
+    rng = np.random.default_rng(7)
+    from tests.test_oracle import _stream
+    run_compare(plan, "cs16le", [_stream("cs16le", plan.new_samples, rng) for _ in range(3)])
+
+
 def test_c5_shape_complex_channelizer():
     """The large complex channelizer: cs16 input, forward FFT 2^20 (two-pass),
     2048 channels of 64..8192, B = 8 — one buffer against the FP64 oracle,
