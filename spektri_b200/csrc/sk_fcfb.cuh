@@ -114,17 +114,31 @@ __device__ __forceinline__ void twiddle_dft(float2* v, const float2* __restrict_
   DftLeaf<R, DIR>::run(v, leaf);
 }
 
+// The threads and the barrier a tile pipeline runs on: the whole CTA
+// (threadIdx.x, __syncthreads), or one 256-thread half of a 512-thread CTA
+// (named barrier 1 + half), so that two halves run independent tiles.
+struct CtaCtx {
+  __device__ __forceinline__ int tid() const { return threadIdx.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct HalfCtx {
+  int t, bar;                                    // thread index in the half; named barrier id
+  __device__ __forceinline__ int tid() const { return t; }
+  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, 256;" ::"r"(bar) : "memory"); }
+};
+
 // Stage 1 (span L = 1): butterfly q of transform t takes inputs
 // i = q + s n/R (load(t, q, s), s = 0..R-1 compile-time after unrolling) and
 // writes y[q R + u]; as the only stage (n = R, q = 0) it stores output u
 // through store(t, 0, u).
-template <int LOGN, int R, int S, int T, int DIR, bool LAST, bool UNROLL, class Load, class Store>
-__device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, Store& store) {
+template <int LOGN, int R, int S, int T, int DIR, bool LAST, bool UNROLL, class Load, class Store,
+          class Ctx = CtaCtx>
+__device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, Store& store, const Ctx& ctx = Ctx()) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   static_assert(NB >= 1, "radix too large for the tile");
 #pragma unroll (UNROLL ? NB : 1)
   for (int bb = 0; bb < NB; ++bb) {
-    const int beta = threadIdx.x + bb * T;
+    const int beta = ctx.tid() + bb * T;
     const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
     float2 v[R];
     if (t < count) {
@@ -150,9 +164,10 @@ __device__ __forceinline__ void stage_first(float2* sm, int count, Load& load, S
 // Stages 2..: span L = 2^LOGL (LOGL = 0: a first stage run from shared
 // memory, in place).  LAST: q < L, g = 0, output o = q + u L stored through
 // store(t, q, u, v) (u compile-time after unrolling).
-template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store, class Pad = PadX>
+template <int LOGN, int R, int LOGL, int S, int T, int DIR, bool LAST, class Store, class Pad = PadX,
+          class Ctx = CtaCtx>
 __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* __restrict__ tw, Store& store,
-                                           const Pad& pad = Pad()) {
+                                           const Pad& pad = Pad(), const Ctx& ctx = Ctx()) {
   constexpr int LOGR = ilog2c(R), LOGNR = LOGN - LOGR, NB = S / (R * T);
   constexpr int SH = TILE_LOGS - LOGL - LOGR;            // stage tables: P = 2^(LOGL + LOGR)
   // SH = -1: the span-4096 radix-4 stage of a 16384-point transform, whose
@@ -165,7 +180,7 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
   if constexpr (LAST) {
 #pragma unroll 1
     for (int bb = 0; bb < NB; ++bb) {
-      const int beta = threadIdx.x + bb * T;
+      const int beta = ctx.tid() + bb * T;
       const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
       const int base = t << LOGN;
       float2 v[R];
@@ -181,17 +196,17 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
     float2 v[NB][R];
 #pragma unroll
     for (int bb = 0; bb < NB; ++bb) {
-      const int beta = threadIdx.x + bb * T;
+      const int beta = ctx.tid() + bb * T;
       const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
       const int base = t << LOGN;
 #pragma unroll
       for (int s = 0; s < R; ++s) v[bb][s] = sm[pad(base + q + (s << LOGNR))];
       twiddled_dft(v[bb], q & ((1 << LOGL) - 1));
     }
-    __syncthreads();
+    ctx.sync();
 #pragma unroll
     for (int bb = 0; bb < NB; ++bb) {
-      const int beta = threadIdx.x + bb * T;
+      const int beta = ctx.tid() + bb * T;
       const int t = beta >> LOGNR, q = beta & ((1 << LOGNR) - 1);
       const int j = q & ((1 << LOGL) - 1), g = q >> LOGL;
       const int ob = (t << LOGN) + (g << (LOGL + LOGR)) + j;
@@ -203,30 +218,30 @@ __device__ __forceinline__ void stage_next(float2* sm, int count, const float2* 
 
 // The whole transform of every tile entry.  The caller syncs before (shared
 // memory free) and after (if it reuses shared memory).
-template <int LOGN, int S, int T, int DIR, bool UNROLL, class Load, class Store>
+template <int LOGN, int S, int T, int DIR, bool UNROLL, class Load, class Store, class Ctx = CtaCtx>
 __device__ __forceinline__ void tile_pipeline(float2* sm, int count, const float2* __restrict__ tw, Load& load,
-                                              Store& store) {
+                                              Store& store, const Ctx& ctx = Ctx()) {
   using P = StagePlan<LOGN, S / T>;
   if constexpr (P::ns == 1) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, true, UNROLL>(sm, count, load, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, true, UNROLL>(sm, count, load, store, ctx);
   } else if constexpr (P::ns == 2) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, true>(sm, count, tw, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store, ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, true>(sm, count, tw, store, PadX(), ctx);
   } else if constexpr (P::ns == 3) {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, true>(sm, count, tw, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store, ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store, PadX(), ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, true>(sm, count, tw, store, PadX(), ctx);
   } else {
-    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, store);
-    __syncthreads();
-    stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, true>(sm, count, tw, store);
+    stage_first<LOGN, 1 << P::r0, S, T, DIR, false, UNROLL>(sm, count, load, store, ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r1, P::r0, S, T, DIR, false>(sm, count, tw, store, PadX(), ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r2, P::r0 + P::r1, S, T, DIR, false>(sm, count, tw, store, PadX(), ctx);
+    ctx.sync();
+    stage_next<LOGN, 1 << P::r3, P::r0 + P::r1 + P::r2, S, T, DIR, true>(sm, count, tw, store, PadX(), ctx);
   }
 }
 
@@ -327,15 +342,16 @@ __device__ __forceinline__ void fcfb_keep(int q, int u, Emit emit) {
   }
 }
 
-template <int LOGN, int S, int T>
-__device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c) {
+template <int LOGN, int S, int T, class Ctx = CtaCtx>
+__device__ __forceinline__ void fcfb_tile(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c,
+                                          const Ctx& ctx = Ctx()) {
   using P = StagePlan<LOGN, S / T>;
   constexpr int R0 = 1 << P::r0, RL = 1 << P::last;
   auto load = [&](int t, int q, int s) { return fcfb_input<LOGN, R0>(meta[t], q, s); };
   auto store = [&](int t, int q, int u, float2 v) {
     fcfb_keep<LOGN, RL>(q, u, [&](int k) { meta[t].out[k] = v; });
   };
-  tile_pipeline<LOGN, S, T, +1, true>(sm, count, c.tw, load, store);
+  tile_pipeline<LOGN, S, T, +1, true>(sm, count, c.tw, load, store, ctx);
 }
 
 // v times e^{+2 pi i k/P} for a runtime k < P (P <= 8): exact swaps and

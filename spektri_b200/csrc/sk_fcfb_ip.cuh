@@ -42,9 +42,9 @@ struct IpPlan {
 // load(t, q, s): input i = q + NL s of transform t.  store(t, kk, u, v):
 // output o = kk + (n/R1) u (the Stockham stores' convention).  count
 // transforms (t < count); the caller syncs before (shared memory free).
-template <int LOGN, int S, int T, class Load, class Store>
+template <int LOGN, int S, int T, class Load, class Store, class Ctx = CtaCtx>
 __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2* __restrict__ tw, Load& load,
-                                            Store& store) {
+                                            Store& store, const Ctx& ctx = Ctx()) {
   using P = IpPlan<LOGN>;
   constexpr int R2 = 1 << P::r_mid, R1 = 1 << P::r_last, LOGNL = LOGN - 4;
   constexpr int NB0 = S / (16 * T), NB1 = S / (R2 * T), NB2 = S / (R1 * T);
@@ -52,7 +52,7 @@ __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2*
   // leaf: 16-point DFTs straight from the loads, stored down a column
 #pragma unroll
   for (int bb = 0; bb < NB0; ++bb) {
-    const int beta = threadIdx.x + bb * T;
+    const int beta = ctx.tid() + bb * T;
     const int t = beta >> LOGNL, q = beta & (P::NL - 1);
     float2 v[16];
     if (t < count) {
@@ -67,7 +67,7 @@ __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2*
 #pragma unroll
     for (int k = 0; k < 16; ++k) p[k * P::ROW] = v[k];
   }
-  __syncthreads();
+  ctx.sync();
   // middle: (i1, k3) per butterfly, k3 fastest across lanes; in place
   {
     constexpr int SH = TILE_LOGS - 4 - P::r_mid;           // table of P = 16 R2, span 16
@@ -75,7 +75,7 @@ __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2*
     float2* base[NB1];
 #pragma unroll
     for (int bb = 0; bb < NB1; ++bb) {
-      const int beta = threadIdx.x + bb * T;
+      const int beta = ctx.tid() + bb * T;
       const int k3 = beta & 15, i1 = (beta >> 4) & (R1 - 1), t = beta >> (4 + P::r_last);
       base[bb] = sm + t * P::SPAN + i1 + P::ROW * k3;
 #pragma unroll
@@ -88,14 +88,14 @@ __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2*
       for (int u = 0; u < R2; ++u) base[bb][R1 * u] = v[bb][u];
     }
   }
-  __syncthreads();
+  ctx.sync();
   // last: k'' per butterfly (k3 fastest), reads a row segment, stores outputs
   {
     constexpr int SH = TILE_LOGS - LOGN;                    // table of P = n, span n/R1
     constexpr int LOGK = LOGN - P::r_last;
 #pragma unroll
     for (int bb = 0; bb < NB2; ++bb) {
-      const int beta = threadIdx.x + bb * T;
+      const int beta = ctx.tid() + bb * T;
       const int kk = beta & ((1 << LOGK) - 1), t = beta >> LOGK;
       const float2* p = sm + t * P::SPAN + R1 * (kk >> 4) + P::ROW * (kk & 15);
       float2 v[R1];
@@ -113,14 +113,15 @@ __device__ __forceinline__ void ip_pipeline(float2* sm, int count, const float2*
 // The filter-bank tile of n = 512 .. 4096 points on the in-place pipeline:
 // input buf[i] = W[j] bin(first + j), j = (i + n/2) mod n (fcfb.rs:166-172),
 // outputs [n/8, 7(n/8)) kept (fcfb.rs:177).
-template <int LOGN, int S, int T>
-__device__ __forceinline__ void fcfb_tile_ip(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c) {
+template <int LOGN, int S, int T, class Ctx = CtaCtx>
+__device__ __forceinline__ void fcfb_tile_ip(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c,
+                                             const Ctx& ctx = Ctx()) {
   constexpr int R1 = 1 << IpPlan<LOGN>::r_last;
   auto load = [&](int t, int q, int s) { return fcfb_input<LOGN, 16>(meta[t], q, s); };
   auto store = [&](int t, int kk, int u, float2 v) {
     fcfb_keep<LOGN, R1>(kk, u, [&](int k) { meta[t].out[k] = v; });
   };
-  ip_pipeline<LOGN, S, T>(sm, count, c.tw, load, store);
+  ip_pipeline<LOGN, S, T>(sm, count, c.tw, load, store, ctx);
 }
 
 // The same in-place scheme for n = 8192 = 16 * 16 * 16 * 2 (one transform
@@ -214,8 +215,26 @@ __device__ __forceinline__ void fcfb_tile_part_ip(float2* sm, const TileMeta* me
   }
 }
 
+// An 8192-point tile of n <= 4096 points in a 512-thread CTA: each 256-thread
+// half runs the first or second half of the tile's transforms as a 4096-point
+// tile of its own, in its own half of shared memory, synchronised by its own
+// named barrier, so that barriers span 8 warps as in the 4096 x 256 shape
+// while 8192-point transforms still run on the whole CTA.
+template <int LOGN>
+__device__ __forceinline__ void fcfb_tile_halves(float2* sm, const TileMeta* meta, int count, const FcfbTileConst& c) {
+  constexpr int HALF = 4096 >> LOGN;                         // transforms per half
+  const int h = threadIdx.x >> 8;
+  const int cnt = min(HALF, count - h * HALF);
+  if (cnt <= 0) return;                                      // this half has nothing (a short tile)
+  const HalfCtx ctx{(int)(threadIdx.x & 255), 1 + h};
+  float2* smh = sm + h * (4096 + 256);
+  if constexpr (LOGN >= 9) fcfb_tile_ip<LOGN, 4096, 256>(smh, meta + h * HALF, cnt, c, ctx);
+  else fcfb_tile<LOGN, 4096, 256>(smh, meta + h * HALF, cnt, c, ctx);
+}
+
 // Filter-bank tile of log2 size log2n (or a chirp-z tile).  With 16 elements
-// per thread, n = 512 .. 4096 run on the in-place pipeline, n = 8192 natively
+// per thread, n = 512 .. 4096 run on the in-place pipeline (in the 8192 x 512
+// shape as two independent 256-thread halves), n = 8192 natively
 // in an 8192-point tile (as two parts in a 4096-point one) and n > S as parts
 // of S points on the in-place pipeline; smaller n, the 32-element shape and
 // the chirp-z tiles run on the Stockham stages (M = 16384 chirp-z tiles in a
@@ -248,6 +267,21 @@ __device__ __forceinline__ void fcfb_tile_dispatch(int log2n, float2* sm, const 
         case 3: if constexpr (IP) fcfb_tile_part_ip<S, T, 3>(sm, meta, c); else fcfb_tile_part<S, T, 3>(sm, meta, c); break;
       }
       return;
+    }
+    if constexpr (S == 8192 && T == 512) {                 // n <= 4096: two independent halves
+      switch (log2n) {
+        case 2: fcfb_tile_halves<2>(sm, meta, count, c); return;
+        case 3: fcfb_tile_halves<3>(sm, meta, count, c); return;
+        case 4: fcfb_tile_halves<4>(sm, meta, count, c); return;
+        case 5: fcfb_tile_halves<5>(sm, meta, count, c); return;
+        case 6: fcfb_tile_halves<6>(sm, meta, count, c); return;
+        case 7: fcfb_tile_halves<7>(sm, meta, count, c); return;
+        case 8: fcfb_tile_halves<8>(sm, meta, count, c); return;
+        case 9: fcfb_tile_halves<9>(sm, meta, count, c); return;
+        case 10: fcfb_tile_halves<10>(sm, meta, count, c); return;
+        case 11: fcfb_tile_halves<11>(sm, meta, count, c); return;
+        case 12: fcfb_tile_halves<12>(sm, meta, count, c); return;
+      }
     }
     switch (log2n) {
       case 2: fcfb_tile<2, S, T>(sm, meta, count, c); break;
