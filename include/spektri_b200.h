@@ -298,6 +298,27 @@ int sk_ddc_process_device(sk_ddc* ddc, const float* in_c64, uint64_t n_in, float
                           void* stream);
 void sk_ddc_destroy(sk_ddc* ddc);
 
+/* ------------------------------------------------------------ post-detection stages
+ * The demodulators' last stages after the downconverters, on one stream of
+ * device samples (tools/demodulator.py):
+ *   SK_AGC_SSB          complex64 in, complex64 out: SsbAgc.execute (:16-65)
+ *   SK_AGC_AM           float32 in, float32 out: AmAgc.execute (:68-103)
+ *   SK_AGC_AM_ENVELOPE  complex64 in, float32 out: |s| (AmDemodulator.execute,
+ *                       :162) followed by AmAgc
+ *   SK_ENVELOPE         complex64 in, float32 out: |s| alone (the AM
+ *                       demodulator without its gain control)
+ * sk_agc_process_device writes n outputs for n inputs; the gain control's
+ * average amplitude carries across calls (0 at creation, as the reference's
+ * constructors set it).  One caller thread per object. */
+#define SK_AGC_SSB 1
+#define SK_AGC_AM 2
+#define SK_AGC_AM_ENVELOPE 3
+#define SK_ENVELOPE 4
+typedef struct sk_agc sk_agc;
+int sk_agc_create(int32_t kind, int32_t device, sk_agc** out);
+int sk_agc_process_device(sk_agc* agc, const float* in, uint64_t n, float* out, void* stream);
+void sk_agc_destroy(sk_agc* agc);
+
 /* Pinned host memory for staging (cudaHostAlloc); NULL on failure. */
 void* sk_host_alloc(size_t bytes);
 void sk_host_free(void* p);

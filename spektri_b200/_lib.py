@@ -23,6 +23,7 @@ SK_ERR_STATE = -7
 
 SPEC_U8, SPEC_U16, SPEC_F32 = 0, 1, 2
 MODE_PLAIN, MODE_BATCHED = 0, 1
+AGC_SSB, AGC_AM, AGC_AM_ENVELOPE, ENVELOPE = 1, 2, 3, 4
 
 
 class SpektriError(RuntimeError):
@@ -106,6 +107,9 @@ PROTOTYPES = [
     ("sk_ddc_process_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64),
                                         C.c_void_p]),
     ("sk_ddc_destroy", None, [C.c_void_p]),
+    ("sk_agc_create", C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("sk_agc_process_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("sk_agc_destroy", None, [C.c_void_p]),
     ("sk_host_alloc", C.c_void_p, [C.c_size_t]),
     ("sk_host_free", None, [C.c_void_p]),
 ]

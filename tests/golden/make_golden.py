@@ -17,6 +17,11 @@ Fixtures:
   ddc_ref.npz            outputs of tools/ddc.py:51-177 (RationalDdc designed by
                          DesignDdc, imported and run here; needs numba and scipy)
                          on seeded complex streams fed in uneven chunks
+  demod_ref.npz          outputs of tools/demodulator.py:106-197 (SsbDemodulator,
+                         AmDemodulator, IqDemodulator with their gain controls,
+                         imported and run here; needs numba and scipy) on the
+                         seeded streams of oracle/demod64.py's CASES, fed in
+                         uneven chunks
 """
 import importlib.util
 import json
@@ -167,6 +172,33 @@ def ddc_ref():
     np.savez_compressed(os.path.join(OUT, "ddc_ref.npz"), **out)
 
 
+def demod_ref():
+    """Demodulator outputs of the reference (tools/demodulator.py) on the
+    seeded streams of oracle/demod64.py's CASES, fed in uneven chunks; each
+    RationalDdc stage's output buffer holds 1000 samples per call
+    (ddc.py:105), so chunks stay below 1000 * decimation / interpolation of
+    the first stage."""
+    sys.path.insert(0, os.path.join(REF, "tools"))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(OUT)))
+    import demodulator
+    from oracle import demod64
+    out = {}
+    for i, case in enumerate(demod64.CASES):
+        d = demod64.make(case, {"ssb": demodulator.SsbDemodulator, "am": demodulator.AmDemodulator,
+                                "iq": demodulator.IqDemodulator})
+        x = demod64.stimulus(case)
+        first = d.ddc
+        limit = max(1, 1000 * first.decimation // first.interpolation - 1)
+        ys, pos, k = [], 0, 0
+        while pos < len(x):
+            c = min(len(x) - pos, limit, [517, 1999, 64, 3001, 1][k % 5])
+            ys.append(np.array(d.execute(x[pos:pos + c])))
+            pos += c
+            k += 1
+        out[f"out{i}"] = np.concatenate(ys)
+    np.savez_compressed(os.path.join(OUT, "demod_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     if not REF or not os.path.isdir(os.path.join(REF, "spektri")):
         sys.exit("usage: make_golden.py <reference root>  (or set SPEKTRI_REFERENCE): the tejeez/spektri tree")
@@ -178,4 +210,5 @@ if __name__ == "__main__":
         json.dump(wire_topics(), f, indent=1)
     proto_fcfb()
     ddc_ref()
+    demod_ref()
     print("golden fixtures written to", OUT)
