@@ -484,11 +484,15 @@ __global__ void __launch_bounds__(T, 2) fwd_rowmix_kernel(FwdArgs a, const float
 // divisions.  Kernels are instantiated for both, so the power-of-two sizes
 // pay nothing for the others.
 template <bool POW2>
-__device__ __forceinline__ float2 z_at(const SplitArgs& a, const float2* Zb, int m) {
-  if (a.R1 == 1) return __ldg(&Zb[m]);
-  if constexpr (POW2) return __ldg(&Zb[((m & (a.R1 - 1)) << a.logM) + (m >> a.log2R1)]);
+__device__ __forceinline__ int z_index(const SplitArgs& a, int m) {
+  if (a.R1 == 1) return m;
+  if constexpr (POW2) return ((m & (a.R1 - 1)) << a.logM) + (m >> a.log2R1);
   const int k2 = m / a.R1;
-  return __ldg(&Zb[((m - k2 * a.R1) << a.logM) + k2]);
+  return ((m - k2 * a.R1) << a.logM) + k2;
+}
+template <bool POW2>
+__device__ __forceinline__ float2 z_at(const SplitArgs& a, const float2* Zb, int m) {
+  return __ldg(&Zb[z_index<POW2>(a, m)]);
 }
 // Real-input bin k in [0, N/2] from the N/2-point complex FFT of the packed
 // pairs: X = (A + B)/2 - i W_N^k (A - B)/2 with A = Z[k mod Nc], B = conj(Z[(Nc-k) mod Nc]).
@@ -556,6 +560,86 @@ __device__ __forceinline__ void store_ext(float2* __restrict__ row, int N, int m
   }
 }
 
+// One bin kk of the spectrum being formed, resolved once for every block of
+// a buffer (the Welch kernels' lanes keep their bin across blocks):
+// get_bin(X, N, kk) is the packed element at ia for complex input, and for
+// real input the split of the elements at ia and ib with twiddle tw,
+// conjugated (sg = -1) when kk mod N mirrors a bin of [0, N/2].  Its
+// extended-row slots: kk, kk + N when below end = N + maxn, and for real
+// 0 < kk < N/2 the conjugate at N - kk and 2N - kk when below end; more
+// copies (maxn > N) take the general loops.
+struct LaneBin {
+  int ia, ib;
+  float2 tw;
+  float sg;
+  bool wrap, mir1, mir2, more;
+};
+
+template <bool REAL, bool POW2>
+__device__ __forceinline__ LaneBin lane_bin(const SplitArgs& a, int maxn, int kk) {
+  int m;
+  if constexpr (POW2) {
+    m = kk & (a.N - 1);
+  } else {
+    m = kk % a.N;
+    m += m < 0 ? a.N : 0;
+  }
+  LaneBin L;
+  L.ib = 0;
+  L.tw = make_float2(0.f, 0.f);
+  L.sg = 1.f;
+  if constexpr (!REAL) {
+    L.ia = z_index<POW2>(a, m);
+  } else {
+    const bool mirror = m >= a.K;
+    const int k = mirror ? a.N - m : m;                      // k in [0, N/2]
+    if constexpr (POW2) {
+      L.ia = z_index<true>(a, k & (a.Nc - 1));
+      L.ib = z_index<true>(a, (a.Nc - k) & (a.Nc - 1));
+    } else {
+      L.ia = z_index<false>(a, k == a.Nc ? 0 : k);
+      L.ib = z_index<false>(a, k == 0 ? 0 : a.Nc - k);
+    }
+    L.tw = __ldg(&a.tw_big[k]);
+    L.sg = mirror ? -1.f : 1.f;
+  }
+  const int end = a.N + maxn;
+  L.wrap = kk + a.N < end;
+  L.mir1 = REAL && kk > 0 && 2 * kk < a.N;
+  L.mir2 = L.mir1 && 2 * a.N - kk < end;
+  L.more = kk + 2 * a.N < end || (L.mir1 && 3 * a.N - kk < end);
+  return L;
+}
+
+// The lane's bin of one block, the same arithmetic as xr_at / x_at.
+template <bool REAL>
+__device__ __forceinline__ float2 lane_x(const LaneBin& L, const float2* __restrict__ Zb) {
+  const float2 za = __ldg(&Zb[L.ia]);
+  if constexpr (!REAL) return za;
+  const float2 zb = cconj(__ldg(&Zb[L.ib]));
+  const float2 s = cadd(za, zb), d = csub(za, zb);
+  const float2 u = cmul(L.tw, d);
+  return make_float2(0.5f * s.x + 0.5f * u.y, L.sg * (0.5f * s.y - 0.5f * u.x));
+}
+
+// store_ext for the lane's bin kk (kk < K) with its slots resolved.
+template <bool REAL>
+__device__ __forceinline__ void lane_store(const LaneBin& L, float2* __restrict__ row, int N, int end, int kk,
+                                           float2 x) {
+  row[kk] = x;
+  if (L.wrap) row[kk + N] = x;
+  if constexpr (REAL) {
+    const float2 c = cconj(x);
+    if (L.mir1) row[N - kk] = c;
+    if (L.mir2) row[2 * N - kk] = c;
+  }
+  if (L.more) {
+    for (int m = kk + 2 * N; m < end; m += N) row[m] = x;
+    if (REAL && L.mir1)
+      for (int m = 3 * N - kk; m < end; m += N) row[m] = cconj(x);
+  }
+}
+
 template <bool REAL>
 __global__ void __launch_bounds__(256) extend_kernel(const float2* __restrict__ X, int K, int N, float2* Xe,
                                                      long long xs, int maxn) {
@@ -602,11 +686,14 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
   const int kk = k0 - 1 + lane;                              // bin this lane forms
   const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
   const int slot = lane - 1;                                 // owner's column in `terms`
-  const SplitArgs& s = a.s;
-  float2* __restrict__ X = s.X;
+  const int N = a.s.N, end = N + a.maxn;
+  const long long zs = a.s.Nc, xs = a.xs;
+  const float2* __restrict__ Z = a.s.Z;
+  float2* __restrict__ X = a.s.X;
+  const LaneBin lb = lane_bin<REAL, POW2>(a.s, a.maxn, kk);
   // Phase B state: thread t sums bin k0 + t.
   const int kb = k0 + threadIdx.x;
-  const bool summer = threadIdx.x < CB && kb < s.K;
+  const bool summer = threadIdx.x < CB && kb < a.s.K;
   float acc = summer ? a.acc[kb] : 0.0f;
   int cnt = a.accn0, r = 0;
   for (int b0 = 0; b0 < a.B; b0 += WELCH_CHUNK) {
@@ -614,25 +701,29 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_kernel(WelchArgs a) {
     // Phase A: warp w forms blocks w, w + WARPS, ... (independent loads).
 #pragma unroll 4
     for (int i = wid; i < nb; i += WELCH_WARPS) {
-      const float2* Zb = s.Z + (size_t)(b0 + i) * s.Nc;
-      const float2 x1 = x_at<REAL, POW2>(s, Zb, kk);
+      const float2 x1 = lane_x<REAL>(lb, Z + (b0 + i) * zs);
       const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
       const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
       if (owner) {
-        store_ext<REAL>(X + (size_t)(b0 + i) * a.xs, s.N, a.maxn, kk, x1);
+        lane_store<REAL>(lb, X + (b0 + i) * xs, N, end, kk, x1);
         const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
         terms[i][slot] = __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
       }
     }
     __syncthreads();
-    // Phase B: accumulate in block order and emit records.
-    for (int i = 0; i < nb; ++i) {
-      if (summer) acc += terms[i][threadIdx.x];
-      if (++cnt >= a.averages) {
-        if (summer) emit_record(a, r, kb, acc, cnt);
-        acc = 0.0f;
-        cnt = 0;
-        ++r;
+    // Phase B: accumulate in block order, one run of additions per record.
+    if (summer) {
+      for (int i = 0; i < nb;) {
+        const int stop = min(nb, i + (a.averages - cnt));
+        cnt += stop - i;
+#pragma unroll 8
+        for (; i < stop; ++i) acc += terms[i][threadIdx.x];
+        if (cnt >= a.averages) {
+          emit_record(a, r, kb, acc, cnt);
+          acc = 0.0f;
+          cnt = 0;
+          ++r;
+        }
       }
     }
     __syncthreads();
@@ -654,17 +745,20 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
   if (k0 >= a.s.K) return;                                   // whole warp: no shuffle partner left behind
   const int kk = k0 - 1 + lane;
   const bool owner = lane >= 1 && lane <= CB && kk < a.s.K;
-  const SplitArgs& s = a.s;
+  const int N = a.s.N, end = N + a.maxn;
+  const long long zs = a.s.Nc, xs = a.xs;
+  const float2* __restrict__ Z = a.s.Z;
+  float2* __restrict__ X = a.s.X;
+  const LaneBin lb = lane_bin<REAL, POW2>(a.s, a.maxn, kk);
   float acc = owner ? a.acc[kk] : 0.0f;
   int cnt = a.accn0, r = 0;
 #pragma unroll 4
   for (int b = 0; b < a.B; ++b) {
-    const float2* Zb = s.Z + (size_t)b * s.Nc;
-    const float2 x1 = x_at<REAL, POW2>(s, Zb, kk);
+    const float2 x1 = lane_x<REAL>(lb, Z + b * zs);
     const float2 x0 = make_float2(__shfl_up_sync(0xffffffffu, x1.x, 1), __shfl_up_sync(0xffffffffu, x1.y, 1));
     const float2 x2 = make_float2(__shfl_down_sync(0xffffffffu, x1.x, 1), __shfl_down_sync(0xffffffffu, x1.y, 1));
     if (owner) {
-      store_ext<REAL>(s.X + (size_t)b * a.xs, s.N, a.maxn, kk, x1);
+      lane_store<REAL>(lb, X + b * xs, N, end, kk, x1);
       const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
       acc += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
     }
