@@ -4,7 +4,9 @@ tejeez/spektri on NVIDIA B200 (sm_100a).
 The compute path is libspektri_b200.so (hand-written CUDA kernels behind a C
 ABI, include/spektri_b200.h); this package is its Python face: ``Plan`` (the
 device filter bank), the reference-shaped ``dsp`` module, the differentiable
-filter-bank stage (``autograd``) and the workload generators.
+filter-bank stage (``autograd``), the workload generators, and the stages
+downstream of a channel (``ddc``: the rational downconverter, ``demod``: the
+SSB / AM / IQ demodulators).
 """
 from .plan import Plan, FORMATS, format_code, pinned_empty
 from . import dsp
