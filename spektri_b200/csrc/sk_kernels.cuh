@@ -783,37 +783,56 @@ __global__ void __launch_bounds__(32 * WELCH_WARPS) welch_bins_kernel(WelchArgs 
 // (one pad slot per R1 bins against bank conflicts), and each thread then
 // forms, accumulates and emits its bins (tid + i T) exactly as
 // welch_bins_kernel does, with coalesced spectrum, accumulator and record
-// accesses.  Blocks run in order, one barrier pair per block.
+// accesses.  Blocks run in order through two shared-memory buffers: block
+// b + 1 is copied in asynchronously (cp.async, no registers held) while
+// block b is formed, one barrier per block.
 constexpr int WT_BINS = 1024;
+constexpr int WT_SLOTS = WT_BINS + WT_BINS / 16 + 2;        // bins m0 - 1 .. m0 + WT_BINS, padded
+
+__device__ __forceinline__ void cp_async8(float2* smem, const float2* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <int T>
 __global__ void __launch_bounds__(T) welch_tr_kernel(WelchArgs a) {
   constexpr int PER = WT_BINS / T;
-  __shared__ float2 zs[WT_BINS + WT_BINS / 16 + 2];         // bins m0 - 1 .. m0 + WT_BINS, padded
+  __shared__ float2 zs[2][WT_SLOTS];
   pdl_wait();                                               // Z from the forward FFT
   const SplitArgs& s = a.s;
   const int logR1 = s.log2R1, logW = ilog2c(WT_BINS) - logR1, W = 1 << logW;
   const int m0 = blockIdx.x * WT_BINS, k20 = m0 >> logR1;
   // bin offset o (o = -1 .. WT_BINS) -> slot; one pad slot after every R1 bins
   auto slot = [&](int o) { return 1 + o + ((o + 1) >> logR1); };
-  float acc[PER];
-#pragma unroll
-  for (int i = 0; i < PER; ++i) acc[i] = a.acc[m0 + threadIdx.x + i * T];
-  int cnt = a.accn0, r = 0;
-  for (int b = 0; b < a.B; ++b) {
+  // Block b's R1 row segments and the two halo bins into buf, asynchronously.
+  auto fetch = [&](int b, float2* buf) {
     const float2* Zb = s.Z + (size_t)b * s.Nc;
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int e = threadIdx.x + i * T, k1 = e >> logW, j = e & (W - 1);
-      zs[slot(k1 + (j << logR1))] = __ldg(&Zb[((size_t)k1 << s.logM) + k20 + j]);
+      cp_async8(&buf[slot(k1 + (j << logR1))], &Zb[((size_t)k1 << s.logM) + k20 + j]);
     }
-    if (threadIdx.x == 0) zs[slot(-1)] = z_at<true>(s, Zb, (m0 - 1) & (s.N - 1));
-    if (threadIdx.x == 1) zs[slot(WT_BINS)] = z_at<true>(s, Zb, (m0 + WT_BINS) & (s.N - 1));
-    __syncthreads();
+    if (threadIdx.x == 0) cp_async8(&buf[slot(-1)], &Zb[z_index<true>(s, (m0 - 1) & (s.N - 1))]);
+    if (threadIdx.x == 1) cp_async8(&buf[slot(WT_BINS)], &Zb[z_index<true>(s, (m0 + WT_BINS) & (s.N - 1))]);
+    cp_async_commit();
+  };
+  float acc[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) acc[i] = a.acc[m0 + threadIdx.x + i * T];
+  int cnt = a.accn0, r = 0;
+  if (a.B > 0) fetch(0, zs[0]);
+  for (int b = 0; b < a.B; ++b) {
+    cp_async_wait_all();
+    __syncthreads();            // block b is in zs[b & 1]; every thread is done reading zs[(b + 1) & 1]
+    if (b + 1 < a.B) fetch(b + 1, zs[(b + 1) & 1]);
+    const float2* z = zs[b & 1];
     float2* Xb = s.X + (size_t)b * a.xs;
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int e = threadIdx.x + i * T;
-      const float2 x0 = zs[slot(e - 1)], x1 = zs[slot(e)], x2 = zs[slot(e + 1)];
+      const float2 x0 = z[slot(e - 1)], x1 = z[slot(e)], x2 = z[slot(e + 1)];
       store_ext<false>(Xb, s.N, a.maxn, m0 + e, x1);
       const float cr = x1.x - (x0.x + x2.x) * 0.5f, ci = x1.y - (x0.y + x2.y) * 0.5f;
       acc[i] += __fadd_rn(__fmul_rn(cr, cr), __fmul_rn(ci, ci));
@@ -827,7 +846,6 @@ __global__ void __launch_bounds__(T) welch_tr_kernel(WelchArgs a) {
       cnt = 0;
       ++r;
     }
-    __syncthreads();                                        // zs is rewritten for the next block
   }
 #pragma unroll
   for (int i = 0; i < PER; ++i) a.acc[m0 + threadIdx.x + i * T] = acc[i];
