@@ -30,6 +30,20 @@ def test_every_declared_symbol_is_exported_and_bound():
         assert n in bound, f"{n} has no ctypes prototype"
 
 
+def test_header_constants_match_the_binding():
+    """Every status and kind code the header defines has the same value in
+    the ctypes binding (a drifted constant would select the wrong stage)."""
+    src = open(os.path.join(ROOT, "include", "spektri_b200.h")).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define\s+(SK_[A-Z0-9_]+)\s+(-?\d+)\b", src)}
+    names = {"SK_OK": "SK_OK", "SK_WARN_FILTER": "SK_WARN_FILTER", "SK_ERR_ARG": "SK_ERR_ARG",
+             "SK_ERR_FILTER": "SK_ERR_FILTER", "SK_ERR_CUDA": "SK_ERR_CUDA", "SK_ERR_NOMEM": "SK_ERR_NOMEM",
+             "SK_ERR_TIMEOUT": "SK_ERR_TIMEOUT", "SK_ERR_UNSUPPORTED": "SK_ERR_UNSUPPORTED",
+             "SK_ERR_STATE": "SK_ERR_STATE", "SK_AGC_SSB": "AGC_SSB", "SK_AGC_AM": "AGC_AM",
+             "SK_AGC_AM_ENVELOPE": "AGC_AM_ENVELOPE", "SK_ENVELOPE": "ENVELOPE"}
+    for h, py in names.items():
+        assert defs[h] == getattr(_lib, py), h
+
+
 def test_no_gpu_fails_loudly_without_fallback():
     import torch
     if torch.cuda.is_available():
