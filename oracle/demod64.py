@@ -143,6 +143,17 @@ def stimulus(case):
     return x.astype(np.complex64)
 
 
+def agc_edges():
+    """Edge streams for the gain controls alone: silence (the average
+    amplitude stays 0, outputs 0), an impulse into silence (the SSB clip and
+    the release), and a step from silence (the attack)."""
+    z = np.zeros(64, np.complex64)
+    imp = np.zeros(96, np.complex64)
+    imp[0] = 1 + 1j
+    step = np.concatenate([np.zeros(16), 0.5 * np.exp(2j * np.pi * 0.01 * np.arange(5000))]).astype(np.complex64)
+    return {"silence": z, "impulse": imp, "step": step}
+
+
 def make(case, cls_map):
     """The case's demodulator from cls_map = {"ssb": ..., "am": ..., "iq": ...}."""
     return cls_map[case["kind"]](case["fs_in"], case["fc_in"], case["fc_demod"], case["mode"], case["agc"])

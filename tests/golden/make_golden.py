@@ -21,7 +21,8 @@ Fixtures:
                          AmDemodulator, IqDemodulator with their gain controls,
                          imported and run here; needs numba and scipy) on the
                          seeded streams of oracle/demod64.py's CASES, fed in
-                         uneven chunks
+                         uneven chunks, and of SsbAgc / AmAgc alone on the edge
+                         streams of demod64.agc_edges (silence, impulse, step)
 """
 import importlib.util
 import json
@@ -196,6 +197,13 @@ def demod_ref():
             pos += c
             k += 1
         out[f"out{i}"] = np.concatenate(ys)
+    # the gain controls alone on their edge streams, in two calls each
+    for name, x in demod64.agc_edges().items():
+        h = len(x) // 3
+        ssb, am = demodulator.SsbAgc(), demodulator.AmAgc()
+        env = np.abs(x).astype(np.float32)
+        out[f"agc_ssb_{name}"] = np.concatenate([ssb.execute(x[:h].copy()), ssb.execute(x[h:].copy())])
+        out[f"agc_am_{name}"] = np.concatenate([am.execute(env[:h].copy()), am.execute(env[h:].copy())])
     np.savez_compressed(os.path.join(OUT, "demod_ref.npz"), **out)
 
 

@@ -7,7 +7,8 @@ GPU: the device chains (spektri_b200/demod.py) against the same fixtures and
 the restatement (relative RMS <= 1e-5 over the whole output and over its
 last three quarters, after the gain controls settle), invariance to how the
 stream is cut into calls (bit-exact), and the gain-control stages alone
-across their 4096-sample segments.
+across their 4096-sample segments and on the reference's outputs for
+silence, an impulse and a step (demod64.agc_edges).
 """
 import os
 
@@ -38,13 +39,52 @@ def errors(y, r):
 
 def test_restatement_matches_reference_outputs():
     d = np.load(GOLDEN)
-    assert len(d.files) == len(demod64.CASES)
+    assert len([k for k in d.files if k.startswith("out")]) == len(demod64.CASES)
     for i, case in enumerate(demod64.CASES):
         o = demod64.make(case, demod64.ORACLE)
         y = chunked(o.execute, demod64.stimulus(case), [4096, 333, 1000, 7, 2500])
         r = d[f"out{i}"]
         assert y.shape == r.shape, (i, y.shape, r.shape)
         assert max(errors(y, r)) < 5e-6, (i, errors(y, r))
+
+
+def _edge_check(y, r):
+    if not np.any(r):
+        assert not np.any(y)                                   # silence stays exactly 0
+    else:
+        assert rel_rms(y, r) < TOL, rel_rms(y, r)
+
+
+def test_restatement_gain_controls_on_edge_streams():
+    """SsbAgc / AmAgc alone on silence (the average amplitude stays 0: the
+    reference's pa <= 0 branch gives 0), an impulse into silence (the SSB clip,
+    then release) and a step from silence (attack), each in two calls."""
+    d = np.load(GOLDEN)
+    for name, x in demod64.agc_edges().items():
+        h = len(x) // 3
+        ssb, am = demod64.SsbAgc64(), demod64.AmAgc64()
+        env = np.abs(x.astype(np.complex128))
+        _edge_check(np.concatenate([ssb.execute(x[:h]), ssb.execute(x[h:])]), d[f"agc_ssb_{name}"])
+        _edge_check(np.concatenate([am.execute(env[:h]), am.execute(env[h:])]), d[f"agc_am_{name}"])
+
+
+@pytest.mark.gpu
+def test_gpu_gain_controls_on_edge_streams():
+    """The device gain controls on the same edge streams and calls."""
+    from spektri_b200 import _lib, demod
+    d = np.load(GOLDEN)
+    for name, x in demod64.agc_edges().items():
+        h = len(x) // 3
+        env = np.abs(x).astype(np.float32)
+        ssb, am = demod.Agc(_lib.AGC_SSB), demod.Agc(_lib.AGC_AM)
+        y = np.concatenate([ssb.execute(x[:h]), ssb.execute(x[h:])])
+        assert y.dtype == np.complex64 and y.shape == x.shape
+        _edge_check(y, d[f"agc_ssb_{name}"])
+        ya = np.concatenate([am.execute(env[:h]), am.execute(env[h:])])
+        assert ya.dtype == np.float32 and ya.shape == x.shape
+        _edge_check(ya, d[f"agc_am_{name}"])
+        if name == "impulse":
+            assert abs(np.abs(y[0]) ** 2 - 0.9) < 1e-5          # clipped to |s|^2 = 0.9 (demodulator.py:58-60)
 
 
 @pytest.mark.gpu
